@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark of the template-matching hot path on B200.
+
+Metric: match_template GMAC/s (exact), one MAC = one (output position,
+template pixel) pair, (W-w+1)(H-h+1)*w*h per score map, masked pixels
+included.
+
+Workload (one step): the 1920x1080 u8 blob scene (200 seeded Gaussian blobs
++ U{-8..8} noise) against its 64x64 template (seeded crop + brightness
+offset), all four MatchTemplateMethods, each unmasked and with the binary
+Bernoulli(0.8) mask: eight 1857x1017 f32 score maps, 8 x 7.74e9 MAC. Each rank
+matches its own scene (seed 1 + rank): independent pairs, no collective on
+the data path, weak scaling.
+
+  value      device-resident throughput: inputs already in HBM, CUDA events
+             around each step, L2 flushed (256 MiB write) between steps
+             outside the timed events;
+  e2e        the same step through the reference-shaped API
+             (imageproc_b200.template_matching, host numpy buffers in and
+             out, host<->device copies inside the timed region);
+  roofline   the dominant kernel's algorithmic int8 ops per second (2 per
+             MAC) from CUDA events recorded by the library around every
+             launch of it, against the int8 dense peak (2x the measured bf16
+             dense figure);
+  cpu_baseline  the oracle's restatement of the reference's per-pixel f32
+             loop, rows split over all host threads like rayon, on a bounded
+             band of output rows.
+
+`--impl reference` times that CPU restatement alone as the reference arm.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "match_template GMAC/s (exact)"
+UNIT = "GMAC/s"
+W_IMG, H_IMG, T = 1920, 1080, 64
+WO, HO = W_IMG - T + 1, H_IMG - T + 1
+MAC_PER_MAP = WO * HO * T * T
+VARIANTS = [(m, masked) for masked in (False, True) for m in range(4)]
+MAC_PER_STEP = MAC_PER_MAP * len(VARIANTS)
+WORKLOAD = ("blob_scene 1920x1080 u8, template 64x64, 4 methods x {unmasked, binary mask "
+            "Bernoulli(0.8)}: 8 score maps 1857x1017 f32 per step")
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict | None:
+        rows = []
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) == 6 and parts[0].isdigit():
+                rows.append(parts)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[2 + i] == "Active"})
+        return {"sm_mhz": statistics.median(int(r[0]) for r in rows),
+                "sm_max_mhz": max(int(r[1]) for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64,
+                     device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_sample(scene, target_s: float, threads: int):
+    """Run the oracle's restatement of the reference over a band of rows of
+    each of the eight score maps; returns (MACs, seconds, rows)."""
+    from oracle import oracle as O
+    image, template, mask, _ = scene
+    # size the band from a 1-row probe so the sample lasts about target_s
+    t0 = time.perf_counter()
+    for m, masked in VARIANTS:
+        O.match_reference(image, template, m, mask if masked else None, rows=(0, 1), threads=1)
+    per_row = (time.perf_counter() - t0) / max(threads, 1)
+    rows = int(max(1, min(HO, target_s / max(per_row, 1e-9))))
+    t0 = time.perf_counter()
+    for m, masked in VARIANTS:
+        O.match_reference(image, template, m, mask if masked else None, rows=(0, rows),
+                          threads=threads)
+    dt = time.perf_counter() - t0
+    return rows * WO * T * T * len(VARIANTS), dt, rows
+
+
+def run_reference(args, world, rank):
+    from imageproc_b200 import synthetic
+    from oracle import oracle as O
+    if rank != 0:
+        return
+    threads = O.default_threads()
+    scene = synthetic.blob_scene(seed=1)
+    for _ in range(args.warmup):
+        cpu_reference_sample(scene, 0.2, threads)
+    macs = secs = 0.0
+    rows_used = 0
+    for _ in range(args.steps):
+        m, s, rows_used = cpu_reference_sample(scene, args.ref_step_s, threads)
+        macs += m
+        secs += s
+    value = macs / secs / 1e9
+    sample = (f"{rows_used} of {HO} output rows of each of the 8 score maps per step "
+              f"(oracle restatement of src/template_matching.rs:219-375, rows over {threads} "
+              f"threads like rayon)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from imageproc_b200 import _lib, device, synthetic
+    from imageproc_b200 import template_matching as tm
+
+    image, template, mask, _ = synthetic.blob_scene(seed=1 + rank)
+    dev = torch.device("cuda", local)
+    di = torch.from_numpy(image).to(dev)
+    dt = torch.from_numpy(template).to(dev)
+    dm = torch.from_numpy(mask).to(dev)
+    outs = [torch.empty((HO, WO), dtype=torch.float32, device=dev) for _ in VARIANTS]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for (m, masked), o in zip(VARIANTS, outs):
+            device.match_template_device(di, dt, m, dm if masked else None, mask_is_binary=True,
+                                         precision=tm.Precision.ExactFp64, out=o, stream=stream)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    _lib.profile_collect()
+    _lib.profile_enable(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = _lib.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k in range(args.steps):
+            flush.zero_()  # outside the timed events: L2 starts cold every step
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.launch_count() - launches0
+    barrier(world)
+    _lib.profile_enable(False)
+    kernels = _lib.profile_collect()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ms = max_over_ranks(ms, world)
+    value = world * MAC_PER_STEP * args.steps / (ms / 1e3) / 1e9
+
+    # e2e through the reference-shaped host API (numpy in, numpy out)
+    e2e_steps = max(1, min(args.steps, 10))
+    tm.set_precision(tm.Precision.ExactFp64)
+    for m, masked in VARIANTS[:2]:
+        tm.match_template(image, template, m)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for m, masked in VARIANTS:
+            if masked:
+                tm.match_template_with_mask(image, template, m, mask)
+            else:
+                tm.match_template(image, template, m)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = world * MAC_PER_STEP * e2e_steps / e2e_s / 1e9
+    h2d = len(VARIANTS) * (image.nbytes + template.nbytes) + 4 * mask.nbytes
+    d2h = len(VARIANTS) * WO * HO * 4
+
+    if rank != 0:
+        return
+    pk = peaks()
+    int8_peak_tops = 2.0 * pk["bf16_tflops"]
+    dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["total_ms"]) if kernels else (None, None)
+    roofline = None
+    if dom:
+        per_launch_s = dom["total_ms"] / dom["launches"] / 1e3
+        macs_per_launch = dom["algorithmic_macs"] / dom["launches"]
+        achieved = 2.0 * macs_per_launch / per_launch_s / 1e12
+        traffic = None
+        tf = ROOT / "profiles" / "traffic.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get(dom_name)
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak_tops,
+                    "unit": "TOP/s", "frac": achieved / int8_peak_tops, "traffic": traffic,
+                    "kernel": dom_name, "launch_ms": per_launch_s * 1e3,
+                    "peak_note": (f"int8 dense = 2 x bf16 dense {pk['bf16_tflops']} TFLOP/s "
+                                  f"({pk['source']}, MEASURED_PEAKS.json); achieved counts 2 ops "
+                                  "per algorithmic MAC"),
+                    "hbm_frac": (dom["algorithmic_bytes"] / dom["launches"] / per_launch_s / 1e9)
+                    / pk["hbm_gbs"]}
+    total_kernel_ms = sum(k["total_ms"] for k in kernels.values()) or 1.0
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = O.default_threads()
+        scene = (image, template, mask, None)
+        macs, secs, rows = cpu_reference_sample(scene, args.cpu_sample_s, threads)
+        cpu = {"value": macs / secs / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"{rows} of {HO} output rows of each of the 8 score maps (oracle "
+                          "restatement of the reference's per-pixel f32 loop, rows over "
+                          f"{threads} threads like rayon), {secs:.1f} s")}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "l2": "flushed between steps (256 MiB write)",
+                   "precision": "exact integer sums, FP64 normalisation",
+                   "parallelism": f"independent scenes per GPU x{world}"},
+        "queries_per_s": world * len(VARIANTS) * args.steps / (ms / 1e3),
+        "roofline": roofline,
+        "kernels": {k: {"launches": v["launches"], "total_ms": v["total_ms"],
+                        "share": v["total_ms"] / total_kernel_ms} for k, v in kernels.items()},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample-s", type=float, default=10.0)
+    ap.add_argument("--ref-step-s", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

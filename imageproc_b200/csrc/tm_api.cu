@@ -1,0 +1,436 @@
+// tm_api.cu -- the C ABI (include/imageproc_b200.h): argument checks, device
+// memory, streams and dispatch to the kernels.
+//
+// Each calling thread owns one context per device: a stream for the
+// host-pointer entry points, grow-only device buffers, and an event marking the
+// last use of its scratch memory. Every call waits for that event on its own
+// stream before touching scratch and records it afterwards, so calls from one
+// thread on different streams never overlap on shared scratch.
+#include <atomic>
+#include <cstdio>
+#include <deque>
+#include <mutex>
+#include <vector>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <unordered_map>
+
+#include "tm_common.cuh"
+#include "tm_internal.h"
+
+#define IPB_API extern "C" __attribute__((visibility("default")))
+
+namespace ipb {
+
+// ---- tracing ----------------------------------------------------------------
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<unsigned long long> g_launches_by_kernel[kKernelCount];
+std::atomic<bool> g_profiling{false};
+
+struct TimedLaunch {
+  KernelTimer timer;
+  double macs, bytes;
+};
+struct KernelStats {
+  unsigned long long launches = 0;
+  double ms = 0, macs = 0, bytes = 0;
+};
+std::mutex g_prof_mu;
+std::deque<TimedLaunch> g_pending;         // recorded, not yet collected (stable addresses)
+std::vector<KernelTimer> g_free_timers;    // event pairs for reuse
+KernelStats g_stats[kKernelCount];
+
+void settle_pending_locked() {
+  for (TimedLaunch& t : g_pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(t.timer.end) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, t.timer.begin, t.timer.end) == cudaSuccess && t.timer.kernel >= 0) {
+      KernelStats& k = g_stats[t.timer.kernel];
+      k.launches += 1;
+      k.ms += ms;
+      k.macs += t.macs;
+      k.bytes += t.bytes;
+    }
+    g_free_timers.push_back(t.timer);
+  }
+  g_pending.clear();
+}
+
+KernelTimer* acquire_timer() {
+  if (!g_profiling.load()) return nullptr;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (g_pending.size() > 4096) settle_pending_locked();
+  KernelTimer t;
+  if (!g_free_timers.empty()) {
+    t = g_free_timers.back();
+    g_free_timers.pop_back();
+  } else if (cudaEventCreate(&t.begin) != cudaSuccess || cudaEventCreate(&t.end) != cudaSuccess) {
+    return nullptr;
+  }
+  t.kernel = -1;
+  g_pending.push_back({t, 0.0, 0.0});
+  return &g_pending.back().timer;
+}
+
+void note_timed(KernelTimer* t, double macs, double bytes) {
+  if (!t) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto it = g_pending.rbegin(); it != g_pending.rend(); ++it)
+    if (&it->timer == t) {
+      it->macs = macs;
+      it->bytes = bytes;
+      return;
+    }
+}
+}  // namespace
+
+const char* kernel_name(int id) {
+  static const char* names[kKernelCount] = {
+      "template_prep", "integral_rows", "integral_cols", "exact_cc",
+      "template_sum_f32", "reference_f32", "find_extremes"};
+  return id >= 0 && id < kKernelCount ? names[id] : "unknown";
+}
+
+void count_launch(int id) {
+  g_launches.fetch_add(1);
+  if (id >= 0 && id < kKernelCount) g_launches_by_kernel[id].fetch_add(1);
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int precision_from_env() {
+  const char* v = std::getenv("IPB_PRECISION");
+  if (!v) return IPB_PRECISION_EXACT_FP64;
+  if (!std::strcmp(v, "1") || !std::strcmp(v, "exact_f32")) return IPB_PRECISION_EXACT_F32;
+  if (!std::strcmp(v, "2") || !std::strcmp(v, "reference_f32")) return IPB_PRECISION_REFERENCE_F32;
+  return IPB_PRECISION_EXACT_FP64;
+}
+std::atomic<int> g_precision{precision_from_env()};
+
+ipb_status fail(ipb_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+ipb_status cuda_fail(cudaError_t e, const char* what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  (void)cudaGetLastError();  // clear a sticky non-fatal error so the next call starts clean
+  if (e == cudaErrorMemoryAllocation) return fail(IPB_ERR_OUT_OF_MEMORY, msg);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return fail(IPB_ERR_NO_DEVICE, msg);
+  return fail(IPB_ERR_CUDA, msg);
+}
+
+#define IPB_CUDA(call, what)                         \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Context {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t last = nullptr;  // last use of any scratch buffer below
+  DevBuf scratch, ext_scratch, ext_result, img, tpl, mask, out;
+  void* pinned = nullptr;  // small pinned host block for reduction results
+  ~Context() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    if (last) cudaEventSynchronize(last);
+    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out})
+      if (b->p) cudaFree(b->p);
+    if (pinned) cudaFreeHost(pinned);
+    if (last) cudaEventDestroy(last);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+ipb_status get_ctx(Context** out) {
+  thread_local std::unordered_map<int, std::unique_ptr<Context>> ctxs;
+  int dev = 0;
+  IPB_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  auto it = ctxs.find(dev);
+  if (it != ctxs.end()) {
+    *out = it->second.get();
+    return IPB_OK;
+  }
+  cudaDeviceProp prop;
+  IPB_CUDA(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  if (prop.major != 10)
+    return fail(IPB_ERR_NO_DEVICE, std::string("imageproc_b200 needs an sm_100 (B200) device; device ") +
+                                       std::to_string(dev) + " is " + prop.name);
+  auto c = std::make_unique<Context>();
+  c->device = dev;
+  IPB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  IPB_CUDA(cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming), "cudaEventCreate");
+  IPB_CUDA(cudaMallocHost(&c->pinned, 256), "cudaMallocHost");
+  *out = c.get();
+  ctxs.emplace(dev, std::move(c));
+  return IPB_OK;
+}
+
+// Grow-only device buffer. The old block may still be read by queued work, so
+// wait for the context's last recorded use before freeing it.
+ipb_status ensure(Context* c, DevBuf& b, size_t bytes, bool zero = false) {
+  if (bytes == 0) bytes = 1;
+  if (b.cap >= bytes) return IPB_OK;
+  IPB_CUDA(cudaEventSynchronize(c->last), "cudaEventSynchronize");
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  const size_t cap = align_up(bytes, 1 << 20);
+  IPB_CUDA(cudaMalloc(&b.p, cap), "cudaMalloc");
+  b.cap = cap;
+  if (zero) IPB_CUDA(cudaMemset(b.p, 0, cap), "cudaMemset");
+  return IPB_OK;
+}
+
+// The reference's assertions, in its order: ImageTemplateMask::new checks the
+// mask first (:433-437), then ImageTemplate::new checks width and height
+// (:395-402).
+ipb_status check_match(uint32_t W, uint32_t H, uint32_t w, uint32_t h, bool masked, uint32_t mw,
+                       uint32_t mh, int method) {
+  if (masked && (mw != w || mh != h))
+    return fail(IPB_ERR_MASK_SIZE, "the template and mask must be the same size");
+  if (W < w) return fail(IPB_ERR_TEMPLATE_WIDTH, "image width must be greater than or equal to template width");
+  if (H < h)
+    return fail(IPB_ERR_TEMPLATE_HEIGHT, "image height must be greater than or equal to template height");
+  if (method < 0 || method > 3) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown MatchTemplateMethod");
+  return IPB_OK;
+}
+
+bool host_mask_is_binary(const uint8_t* m, size_t n) {
+  for (size_t k = 0; k < n; ++k)
+    if (m[k] > 1) return false;
+  return true;
+}
+
+// Enqueue one matching problem on a.stream.
+ipb_status run_match(Context* c, const MatchArgs& a) {
+  const size_t out_bytes = (size_t)(a.W - a.w + 1) * (a.H - a.h + 1) * sizeof(float);
+  if (a.w == 0 || a.h == 0) {
+    // empty window: every score is 0 (the walk never runs, :410-416)
+    IPB_CUDA(cudaMemsetAsync(a.out, 0, out_bytes, a.stream), "cudaMemsetAsync");
+    return IPB_OK;
+  }
+  const bool ref = a.precision == IPB_PRECISION_REFERENCE_F32;
+  const size_t need = ref ? reference_scratch_bytes(a) : exact_cc_scratch_bytes(a);
+  ipb_status st = ensure(c, c->scratch, need);
+  if (st) return st;
+  IPB_CUDA(cudaStreamWaitEvent(a.stream, c->last, 0), "cudaStreamWaitEvent");
+  MatchArgs la = a;
+  la.timer = acquire_timer();
+  cudaError_t e = ref ? launch_reference(la, c->scratch.p) : launch_exact_cc(la, c->scratch.p);
+  if (la.timer) {
+    const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
+    note_timed(la.timer, Wo * Ho * tp,
+               (double)a.W * a.H + tp * (a.mask ? 2.0 : 1.0) + 4.0 * Wo * Ho);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "template-matching launch");
+  IPB_CUDA(cudaEventRecord(c->last, a.stream), "cudaEventRecord");
+  return IPB_OK;
+}
+
+ipb_status host_match(const uint8_t* image, uint32_t W, uint32_t H, const uint8_t* tpl, uint32_t w,
+                      uint32_t h, int method, const uint8_t* mask, uint32_t mw, uint32_t mh,
+                      float* out) {
+  ipb_status st = check_match(W, H, w, h, mask != nullptr, mw, mh, method);
+  if (st) return st;
+  if ((!image && (size_t)W * H) || (!tpl && (size_t)w * h) || !out)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  const size_t ib = (size_t)W * H, tb = (size_t)w * h;
+  const size_t ob = (size_t)(W - w + 1) * (H - h + 1) * sizeof(float);
+  if ((st = ensure(c, c->img, ib)) || (st = ensure(c, c->tpl, tb)) || (st = ensure(c, c->out, ob)))
+    return st;
+  if (mask && (st = ensure(c, c->mask, tb))) return st;
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  if (ib) IPB_CUDA(cudaMemcpyAsync(c->img.p, image, ib, cudaMemcpyHostToDevice, c->stream), "copy image");
+  if (tb) IPB_CUDA(cudaMemcpyAsync(c->tpl.p, tpl, tb, cudaMemcpyHostToDevice, c->stream), "copy template");
+  if (mask && tb)
+    IPB_CUDA(cudaMemcpyAsync(c->mask.p, mask, tb, cudaMemcpyHostToDevice, c->stream), "copy mask");
+  MatchArgs a{static_cast<const uint8_t*>(c->img.p), W, H, static_cast<const uint8_t*>(c->tpl.p), w, h,
+              mask ? static_cast<const uint8_t*>(c->mask.p) : nullptr,
+              mask ? host_mask_is_binary(mask, tb) : false, method, g_precision.load(),
+              static_cast<float*>(c->out.p), c->stream};
+  if ((st = run_match(c, a))) return st;
+  IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy scores");
+  IPB_CUDA(cudaEventRecord(c->last, c->stream), "cudaEventRecord");
+  IPB_CUDA(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return IPB_OK;
+}
+
+template <typename T, typename R>
+ipb_status extremes_common(Context* c, const T* d, uint32_t W, uint32_t H, R* out, cudaStream_t s) {
+  using DT = typename std::conditional<
+      std::is_same<T, uint64_t>::value, unsigned long long,
+      typename std::conditional<std::is_same<T, int64_t>::value, long long, T>::type>::type;
+  ipb_status st;
+  if ((st = ensure(c, c->ext_scratch, extremes_scratch_bytes(), /*zero=*/true))) return st;
+  if ((st = ensure(c, c->ext_result, sizeof(ExtremesResult<DT>)))) return st;
+  IPB_CUDA(cudaStreamWaitEvent(s, c->last, 0), "cudaStreamWaitEvent");
+  auto* res = static_cast<ExtremesResult<DT>*>(c->ext_result.p);
+  cudaError_t e = launch_find_extremes<DT>(reinterpret_cast<const DT*>(d), (unsigned long long)W * H,
+                                           c->ext_scratch.p, res, s);
+  if (e != cudaSuccess) return cuda_fail(e, "find_extremes launch");
+  IPB_CUDA(cudaMemcpyAsync(c->pinned, res, sizeof(ExtremesResult<DT>), cudaMemcpyDeviceToHost, s),
+           "copy extremes");
+  IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
+  IPB_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  ExtremesResult<DT> r;
+  std::memcpy(&r, c->pinned, sizeof(r));
+  out->max_value = (T)r.max_value;
+  out->min_value = (T)r.min_value;
+  out->max_value_location_x = (uint32_t)(r.max_index % W);
+  out->max_value_location_y = (uint32_t)(r.max_index / W);
+  out->min_value_location_x = (uint32_t)(r.min_index % W);
+  out->min_value_location_y = (uint32_t)(r.min_index / W);
+  return IPB_OK;
+}
+
+template <typename T, typename R>
+ipb_status extremes_host(const T* image, uint32_t W, uint32_t H, R* out) {
+  if (W == 0 || H == 0) return fail(IPB_ERR_EMPTY_IMAGE, "image must be non-empty");
+  if (!image || !out) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  const size_t bytes = (size_t)W * H * sizeof(T);
+  if ((st = ensure(c, c->img, bytes))) return st;
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(cudaMemcpyAsync(c->img.p, image, bytes, cudaMemcpyHostToDevice, c->stream), "copy image");
+  return extremes_common<T, R>(c, static_cast<const T*>(c->img.p), W, H, out, c->stream);
+}
+
+template <typename T, typename R>
+ipb_status extremes_device(const T* d_image, uint32_t W, uint32_t H, R* out, void* stream) {
+  if (W == 0 || H == 0) return fail(IPB_ERR_EMPTY_IMAGE, "image must be non-empty");
+  if (!d_image || !out) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  return extremes_common<T, R>(c, d_image, W, H, out, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace
+}  // namespace ipb
+
+using namespace ipb;
+
+IPB_API const char* ipb_last_error_message(void) { return g_last_error.c_str(); }
+
+IPB_API const char* ipb_version(void) { return "imageproc_b200 0.1.0 (sm_100a)"; }
+
+IPB_API uint64_t ipb_launch_count(void) { return g_launches.load(); }
+
+IPB_API ipb_status ipb_profile_enable(int enable) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  settle_pending_locked();
+  g_profiling.store(enable != 0);
+  return IPB_OK;
+}
+
+IPB_API int ipb_profile_collect(ipb_kernel_stats* out, int max_entries) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  settle_pending_locked();
+  int n = 0;
+  for (int k = 0; k < kKernelCount; ++k) {
+    if (!g_stats[k].launches) continue;
+    if (out && n < max_entries) {
+      out[n].name = kernel_name(k);
+      out[n].launches = g_stats[k].launches;
+      out[n].total_ms = g_stats[k].ms;
+      out[n].algorithmic_macs = g_stats[k].macs;
+      out[n].algorithmic_bytes = g_stats[k].bytes;
+    }
+    ++n;
+    g_stats[k] = KernelStats{};
+  }
+  return n;
+}
+
+IPB_API ipb_status ipb_set_precision(int precision) {
+  if (precision < 0 || precision > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown precision");
+  g_precision.store(precision);
+  return IPB_OK;
+}
+
+IPB_API int ipb_get_precision(void) { return g_precision.load(); }
+
+IPB_API ipb_status ipb_match_template(const uint8_t* image, uint32_t W, uint32_t H, const uint8_t* tpl,
+                                      uint32_t w, uint32_t h, int method, float* out) {
+  return host_match(image, W, H, tpl, w, h, method, nullptr, 0, 0, out);
+}
+
+IPB_API ipb_status ipb_match_template_parallel(const uint8_t* image, uint32_t W, uint32_t H,
+                                               const uint8_t* tpl, uint32_t w, uint32_t h, int method,
+                                               float* out) {
+  return host_match(image, W, H, tpl, w, h, method, nullptr, 0, 0, out);
+}
+
+IPB_API ipb_status ipb_match_template_with_mask(const uint8_t* image, uint32_t W, uint32_t H,
+                                                const uint8_t* tpl, uint32_t w, uint32_t h, int method,
+                                                const uint8_t* mask, uint32_t mw, uint32_t mh,
+                                                float* out) {
+  if (!mask) return fail(IPB_ERR_INVALID_ARGUMENT, "null mask");
+  return host_match(image, W, H, tpl, w, h, method, mask, mw, mh, out);
+}
+
+IPB_API ipb_status ipb_match_template_with_mask_parallel(const uint8_t* image, uint32_t W, uint32_t H,
+                                                         const uint8_t* tpl, uint32_t w, uint32_t h,
+                                                         int method, const uint8_t* mask, uint32_t mw,
+                                                         uint32_t mh, float* out) {
+  if (!mask) return fail(IPB_ERR_INVALID_ARGUMENT, "null mask");
+  return host_match(image, W, H, tpl, w, h, method, mask, mw, mh, out);
+}
+
+IPB_API ipb_status ipb_match_template_device(const uint8_t* d_image, uint32_t W, uint32_t H,
+                                             const uint8_t* d_tpl, uint32_t w, uint32_t h,
+                                             const uint8_t* d_mask, uint32_t mw, uint32_t mh,
+                                             int mask_is_binary, int method, int precision, float* d_out,
+                                             void* stream) {
+  ipb_status st = check_match(W, H, w, h, d_mask != nullptr, mw, mh, method);
+  if (st) return st;
+  if (precision < 0 || precision > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if ((!d_image && (size_t)W * H) || (!d_tpl && (size_t)w * h) || !d_out)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  MatchArgs a{d_image, W, H, d_tpl, w, h, d_mask, d_mask && mask_is_binary != 0, method, precision, d_out,
+              static_cast<cudaStream_t>(stream)};
+  return run_match(c, a);
+}
+
+#define IPB_DEFINE_FIND_EXTREMES(T, S)                                                            \
+  IPB_API ipb_status ipb_find_extremes_##S(const T* image, uint32_t width, uint32_t height,        \
+                                           ipb_extremes_##S* out) {                                \
+    return extremes_host<T, ipb_extremes_##S>(image, width, height, out);                         \
+  }                                                                                                \
+  IPB_API ipb_status ipb_find_extremes_##S##_device(const T* d_image, uint32_t width,             \
+                                                    uint32_t height, ipb_extremes_##S* out,        \
+                                                    void* stream) {                                \
+    return extremes_device<T, ipb_extremes_##S>(d_image, width, height, out, stream);             \
+  }
+
+IPB_DEFINE_FIND_EXTREMES(uint8_t, u8)
+IPB_DEFINE_FIND_EXTREMES(uint16_t, u16)
+IPB_DEFINE_FIND_EXTREMES(uint32_t, u32)
+IPB_DEFINE_FIND_EXTREMES(uint64_t, u64)
+IPB_DEFINE_FIND_EXTREMES(int8_t, i8)
+IPB_DEFINE_FIND_EXTREMES(int16_t, i16)
+IPB_DEFINE_FIND_EXTREMES(int32_t, i32)
+IPB_DEFINE_FIND_EXTREMES(int64_t, i64)
+IPB_DEFINE_FIND_EXTREMES(float, f32)
+IPB_DEFINE_FIND_EXTREMES(double, f64)

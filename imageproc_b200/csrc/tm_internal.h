@@ -1,0 +1,104 @@
+// tm_internal.h -- launchers shared between the kernel files and the C ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ipb {
+
+// ---- tracing ---------------------------------------------------------------
+// Every kernel launch site reports itself; the C ABI exposes the running
+// count (ipb_launch_count) and, when profiling is on, CUDA-event timings of
+// the dominant kernel of each call (ipb_profile_collect).
+enum KernelId : int {
+  kKernelPrep = 0,
+  kKernelIntegralRows,
+  kKernelIntegralCols,
+  kKernelExactCC,
+  kKernelTemplateSumF32,
+  kKernelReference,
+  kKernelExtremes,
+  kKernelCount
+};
+const char* kernel_name(int id);
+void count_launch(int id);
+
+// Event pair recorded around a call's dominant kernel (both null = off).
+struct KernelTimer {
+  cudaEvent_t begin = nullptr;
+  cudaEvent_t end = nullptr;
+  int kernel = -1;  // set by the launcher: which kernel was timed
+};
+
+// One (image, template[, mask]) matching problem, all pointers on the device.
+struct MatchArgs {
+  const uint8_t* img;
+  uint32_t W, H;
+  const uint8_t* tpl;
+  uint32_t w, h;
+  const uint8_t* mask;  // nullptr when unmasked
+  bool mask_binary;     // every mask value is 0 or 1
+  int method;
+  int precision;
+  float* out;           // (W-w+1) x (H-h+1)
+  cudaStream_t stream;
+  KernelTimer* timer = nullptr;
+};
+
+inline void timer_begin(KernelTimer* t, int kernel, cudaStream_t s) {
+  if (t && t->begin) {
+    t->kernel = kernel;
+    cudaEventRecord(t->begin, s);
+  }
+}
+inline void timer_end(KernelTimer* t, cudaStream_t s) {
+  if (t && t->end) cudaEventRecord(t->end, s);
+}
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// ---- template preparation (tm_prep.cu) ----------------------------------
+// Byte planes of the template-side operands, each h rows of `pitch` bytes,
+// zero beyond w, followed by the u64 template constant TSS.
+//   unmasked: plane 0 = T
+//   binary mask: plane 0 = T*m, plane 1 = m
+//   general mask: planes 0..2 = bytes of T*m^2, planes 3..4 = bytes of m^2
+int template_plane_count(const MatchArgs& a);
+size_t template_pitch(uint32_t w);
+size_t prep_scratch_bytes(const MatchArgs& a);
+cudaError_t launch_prep(const MatchArgs& a, uint8_t* planes, unsigned long long* tss);
+
+// ---- u64 integral image of I^2 (tm_integral.cu) --------------------------
+// Exclusive summed-area table, (H+1) x (W+1) u64, S[y][x] = sum over y'<y,
+// x'<x, the layout of imageproc's integral_squared_image
+// (src/integral_image.rs:11-22, :89).
+size_t integral_bytes(uint32_t W, uint32_t H);
+cudaError_t launch_integral_squared(const uint8_t* img, uint32_t W, uint32_t H,
+                                    unsigned long long* sat, cudaStream_t s);
+cudaError_t launch_integral(const uint8_t* img, uint32_t W, uint32_t H,
+                            unsigned long long* sat, cudaStream_t s);
+
+// ---- CUDA-core exact kernel (tm_exact_cc.cu) ------------------------------
+size_t exact_cc_scratch_bytes(const MatchArgs& a);
+cudaError_t launch_exact_cc(const MatchArgs& a, void* scratch);
+
+// ---- reference-order f32 kernel (tm_reference.cu) -------------------------
+size_t reference_scratch_bytes(const MatchArgs& a);
+cudaError_t launch_reference(const MatchArgs& a, void* scratch);
+
+// ---- find_extremes (tm_extremes.cu) ----------------------------------------
+// Result record written to device memory by the reduction.
+template <typename T>
+struct ExtremesResult {
+  T max_value;
+  T min_value;
+  unsigned long long max_index;
+  unsigned long long min_index;
+};
+size_t extremes_scratch_bytes();
+template <typename T>
+cudaError_t launch_find_extremes(const T* d, unsigned long long n, void* scratch,
+                                 ExtremesResult<T>* d_result, cudaStream_t s);
+
+}  // namespace ipb

@@ -1,0 +1,216 @@
+/*
+ * imageproc_b200.h -- C ABI of the B200 (sm_100a) template-matching library.
+ *
+ * Drop-in boundary for imageproc's template-matching module
+ * (imageproc 0.27.0, src/template_matching.rs). Every entry point below names
+ * the reference item it replaces. Plain pointers and sizes only; every
+ * function returns an ipb_status (0 = success) and, on failure, leaves a
+ * message for ipb_last_error_message().
+ *
+ * Images are the reference's `Image<P>` layout (src/definitions.rs:14):
+ * row-major, stride == width, no padding. Outputs of the match functions are
+ * (width - template_width + 1) x (height - template_height + 1) f32 score maps
+ * (src/template_matching.rs:420-424).
+ *
+ * Host-pointer entry points copy their inputs to the current CUDA device,
+ * run there and copy the result back before returning (synchronous, like the
+ * reference's functions). `_device` entry points take device pointers and a
+ * cudaStream_t (passed as void*, NULL = legacy default stream) and only
+ * enqueue work; results are ready when the stream is.
+ *
+ * There is no CPU fallback: without a usable sm_100 device every compute
+ * entry point fails with IPB_ERR_CUDA or IPB_ERR_NO_DEVICE. Argument checks
+ * run on the host before any device work, in the reference's order.
+ */
+#ifndef IMAGEPROC_B200_H
+#define IMAGEPROC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+typedef enum ipb_status {
+    IPB_OK = 0,
+    /* "image width must be greater than or equal to template width"
+     * (src/template_matching.rs:395-398) */
+    IPB_ERR_TEMPLATE_WIDTH = 1,
+    /* "image height must be greater than or equal to template height"
+     * (src/template_matching.rs:399-402) */
+    IPB_ERR_TEMPLATE_HEIGHT = 2,
+    /* "the template and mask must be the same size"
+     * (src/template_matching.rs:433-437) */
+    IPB_ERR_MASK_SIZE = 3,
+    /* "image must be non-empty" (src/template_matching.rs:483-486) */
+    IPB_ERR_EMPTY_IMAGE = 4,
+    IPB_ERR_INVALID_ARGUMENT = 5,
+    IPB_ERR_CUDA = 6,
+    IPB_ERR_NO_DEVICE = 7,
+    IPB_ERR_OUT_OF_MEMORY = 8,
+    IPB_ERR_TIMEOUT = 9
+} ipb_status;
+
+/* MatchTemplateMethod (src/template_matching.rs:8-64), same order. */
+typedef enum ipb_method {
+    IPB_SUM_OF_SQUARED_ERRORS = 0,
+    IPB_SUM_OF_SQUARED_ERRORS_NORMALIZED = 1,
+    IPB_CROSS_CORRELATION = 2,
+    IPB_CROSS_CORRELATION_NORMALIZED = 3
+} ipb_method;
+
+/* Arithmetic of the score maps.
+ *  EXACT_FP64 (default): exact integer window sums; SSE assembled as
+ *    sum(I^2) - 2 sum(I*T) + sum(T^2); one f32 rounding of the integer score;
+ *    normalised methods divide by sqrt(sum(I^2) * sum(T^2)) in FP64 and
+ *    round once to f32.
+ *  EXACT_F32: exact integer window sums, then the reference's own f32
+ *    normalisation sequence (src/template_matching.rs:249-250).
+ *  REFERENCE_F32: the reference's f32 accumulation order replicated
+ *    (dy-outer, dx-inner sequential f32 sums, src/template_matching.rs:
+ *    219-386), bit-identical to the reference on every input. */
+typedef enum ipb_precision {
+    IPB_PRECISION_EXACT_FP64 = 0,
+    IPB_PRECISION_EXACT_F32 = 1,
+    IPB_PRECISION_REFERENCE_F32 = 2
+} ipb_precision;
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char *ipb_last_error_message(void);
+
+/* Library version string. */
+const char *ipb_version(void);
+
+/* Process-wide precision used by the reference-shaped entry points (the
+ * ones without a precision argument). Default IPB_PRECISION_EXACT_FP64, or
+ * the value of the environment variable IPB_PRECISION (0, 1, 2 or
+ * exact_fp64 / exact_f32 / reference_f32) at load time. */
+ipb_status ipb_set_precision(int precision);
+int ipb_get_precision(void);
+
+/* ---- tracing -------------------------------------------------------------
+ * No counterpart in the reference (which has no instrumentation); used by the
+ * benchmark and the profiling notes. */
+
+/* Number of kernels this library has launched in the process so far. */
+uint64_t ipb_launch_count(void);
+
+/* When enabled, each matching call records CUDA events around its dominant
+ * kernel on the call's stream. */
+ipb_status ipb_profile_enable(int enable);
+
+typedef struct ipb_kernel_stats {
+    const char *name;         /* kernel family */
+    uint64_t launches;        /* timed launches */
+    double total_ms;          /* summed event time of those launches */
+    double algorithmic_macs;  /* summed (W-w+1)(H-h+1)*w*h */
+    double algorithmic_bytes; /* summed image + template (+mask) + f32 output */
+} ipb_kernel_stats;
+
+/* Waits for the recorded events, writes up to max_entries per-kernel records
+ * (those with at least one timed launch), resets the counters and returns
+ * the number of records available. */
+int ipb_profile_collect(ipb_kernel_stats *out, int max_entries);
+
+/* ---- match_template ------------------------------------------------------ */
+
+/* match_template (src/template_matching.rs:78-92). */
+ipb_status ipb_match_template(const uint8_t *image, uint32_t image_width,
+                              uint32_t image_height, const uint8_t *templ,
+                              uint32_t template_width,
+                              uint32_t template_height, int method,
+                              float *out);
+
+/* match_template_parallel (src/template_matching.rs:96-110). The reference
+ * computes the same values as match_template with rows on rayon threads;
+ * here both run the same device path, so results are identical. */
+ipb_status ipb_match_template_parallel(const uint8_t *image,
+                                       uint32_t image_width,
+                                       uint32_t image_height,
+                                       const uint8_t *templ,
+                                       uint32_t template_width,
+                                       uint32_t template_height, int method,
+                                       float *out);
+
+/* match_template_with_mask (src/template_matching.rs:125-140). The mask is a
+ * GrayImage of its own size; its size must equal the template's. Mask values
+ * are arbitrary u8 weights, as in the reference. */
+ipb_status ipb_match_template_with_mask(
+    const uint8_t *image, uint32_t image_width, uint32_t image_height,
+    const uint8_t *templ, uint32_t template_width, uint32_t template_height,
+    int method, const uint8_t *mask, uint32_t mask_width,
+    uint32_t mask_height, float *out);
+
+/* match_template_with_mask_parallel (src/template_matching.rs:144-163). */
+ipb_status ipb_match_template_with_mask_parallel(
+    const uint8_t *image, uint32_t image_width, uint32_t image_height,
+    const uint8_t *templ, uint32_t template_width, uint32_t template_height,
+    int method, const uint8_t *mask, uint32_t mask_width,
+    uint32_t mask_height, float *out);
+
+/* Device-resident form of the four functions above with an explicit
+ * precision. mask may be NULL (unmasked); mask_is_binary != 0 asserts every
+ * mask value is 0 or 1, which selects the cheaper binary-mask plan (a
+ * non-binary mask under that flag gives wrong scores, so pass 0 when in
+ * doubt). Replaces the same reference items as the host forms. */
+ipb_status ipb_match_template_device(
+    const uint8_t *d_image, uint32_t image_width, uint32_t image_height,
+    const uint8_t *d_templ, uint32_t template_width, uint32_t template_height,
+    const uint8_t *d_mask, uint32_t mask_width, uint32_t mask_height,
+    int mask_is_binary, int method, int precision, float *d_out,
+    void *stream);
+
+/* ---- find_extremes -------------------------------------------------------- */
+
+/* Extremes<T> (src/template_matching.rs:463-475), field order kept. */
+#define IPB_DECLARE_EXTREMES(T, S)                                            \
+    typedef struct ipb_extremes_##S {                                         \
+        T max_value;                                                          \
+        T min_value;                                                          \
+        uint32_t max_value_location_x, max_value_location_y;                  \
+        uint32_t min_value_location_x, min_value_location_y;                  \
+    } ipb_extremes_##S;
+
+IPB_DECLARE_EXTREMES(uint8_t, u8)
+IPB_DECLARE_EXTREMES(uint16_t, u16)
+IPB_DECLARE_EXTREMES(uint32_t, u32)
+IPB_DECLARE_EXTREMES(uint64_t, u64)
+IPB_DECLARE_EXTREMES(int8_t, i8)
+IPB_DECLARE_EXTREMES(int16_t, i16)
+IPB_DECLARE_EXTREMES(int32_t, i32)
+IPB_DECLARE_EXTREMES(int64_t, i64)
+IPB_DECLARE_EXTREMES(float, f32)
+IPB_DECLARE_EXTREMES(double, f64)
+
+/* find_extremes<T> (src/template_matching.rs:479-511) for every Primitive
+ * channel type (usize/isize map to the 64-bit forms). Ties resolve to the
+ * first pixel in row-major order; a NaN at (0, 0) is returned for both
+ * extremes, other NaNs are skipped, exactly like the reference's strict
+ * comparisons. Empty images fail with IPB_ERR_EMPTY_IMAGE. */
+#define IPB_DECLARE_FIND_EXTREMES(T, S)                                       \
+    ipb_status ipb_find_extremes_##S(const T *image, uint32_t width,          \
+                                     uint32_t height,                         \
+                                     ipb_extremes_##S *out);                  \
+    ipb_status ipb_find_extremes_##S##_device(const T *d_image,               \
+                                              uint32_t width,                 \
+                                              uint32_t height,                \
+                                              ipb_extremes_##S *out,          \
+                                              void *stream);
+
+IPB_DECLARE_FIND_EXTREMES(uint8_t, u8)
+IPB_DECLARE_FIND_EXTREMES(uint16_t, u16)
+IPB_DECLARE_FIND_EXTREMES(uint32_t, u32)
+IPB_DECLARE_FIND_EXTREMES(uint64_t, u64)
+IPB_DECLARE_FIND_EXTREMES(int8_t, i8)
+IPB_DECLARE_FIND_EXTREMES(int16_t, i16)
+IPB_DECLARE_FIND_EXTREMES(int32_t, i32)
+IPB_DECLARE_FIND_EXTREMES(int64_t, i64)
+IPB_DECLARE_FIND_EXTREMES(float, f32)
+IPB_DECLARE_FIND_EXTREMES(double, f64)
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMAGEPROC_B200_H */

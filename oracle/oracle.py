@@ -1,0 +1,131 @@
+"""ctypes binding of the CPU oracle (``oracle/tm_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA path. Imported by the
+test-suite, the smoke check and the benchmark's CPU-baseline leg, never by
+the ``imageproc_b200`` package.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libtm_oracle.so"
+
+TYPE_CODES = {np.dtype(t): k for k, t in enumerate(
+    ["uint8", "uint16", "uint32", "uint64", "int8", "int16", "int32", "int64", "float32", "float64"])}
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        u8p, f32p, u64p = C.c_void_p, C.c_void_p, C.c_void_p
+        u32 = C.c_uint32
+        L.tmo_match_reference.argtypes = [u8p, u32, u32, u8p, u32, u32, u8p, u32, u32, C.c_int,
+                                          f32p, u32, u32, C.c_int]
+        L.tmo_sums.argtypes = [u8p, u32, u32, u8p, u32, u32, u8p, u64p, u64p, u64p, C.c_int]
+        L.tmo_match_exact.argtypes = [u8p, u32, u32, u8p, u32, u32, u8p, u32, u32, C.c_int, C.c_int,
+                                      f32p, C.c_int]
+        L.tmo_finish.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64]
+        L.tmo_finish.restype = C.c_float
+        L.tmo_find_extremes_index.argtypes = [C.c_void_p, u32, u32, C.c_int,
+                                              C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def default_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+class OracleError(AssertionError):
+    pass
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _dims(image, template, mask):
+    image = np.ascontiguousarray(image, np.uint8)
+    template = np.ascontiguousarray(template, np.uint8)
+    if mask is not None:
+        mask = np.ascontiguousarray(mask, np.uint8)
+    return image, template, mask
+
+
+def match_reference(image, template, method, mask=None, rows=None, threads=None) -> np.ndarray:
+    """The reference's f32 scores (bit-exact restatement). ``rows`` = (begin,
+    end) restricts the output rows (a bounded sample)."""
+    image, template, mask = _dims(image, template, mask)
+    H, W = image.shape
+    h, w = template.shape
+    mh, mw = mask.shape if mask is not None else (0, 0)
+    Ho, Wo = H - h + 1, W - w + 1
+    r0, r1 = rows if rows is not None else (0, Ho)
+    out = np.empty((max(r1 - r0, 0), Wo), np.float32)
+    st = lib().tmo_match_reference(_p(image), W, H, _p(template), w, h, _p(mask), mw, mh,
+                                   int(method), _p(out), r0, r1,
+                                   threads if threads is not None else default_threads())
+    if st:
+        raise OracleError(f"oracle status {st}")
+    return out
+
+
+def sums(image, template, mask=None, threads=None):
+    """Exact (X, Y, TSS) integer sums."""
+    image, template, mask = _dims(image, template, mask)
+    H, W = image.shape
+    h, w = template.shape
+    X = np.empty((H - h + 1, W - w + 1), np.uint64)
+    Y = np.empty_like(X)
+    tss = C.c_uint64()
+    st = lib().tmo_sums(_p(image), W, H, _p(template), w, h, _p(mask), _p(X), _p(Y),
+                        C.byref(tss), threads if threads is not None else default_threads())
+    if st:
+        raise OracleError(f"oracle status {st}")
+    return X, Y, tss.value
+
+
+def match_exact(image, template, method, mask=None, precision=0, threads=None) -> np.ndarray:
+    """Exact integer sums + FP64 (precision 0) or f32 (1) normalisation."""
+    image, template, mask = _dims(image, template, mask)
+    H, W = image.shape
+    h, w = template.shape
+    mh, mw = mask.shape if mask is not None else (0, 0)
+    out = np.empty((H - h + 1, W - w + 1), np.float32)
+    st = lib().tmo_match_exact(_p(image), W, H, _p(template), w, h, _p(mask), mw, mh,
+                               int(method), int(precision), _p(out),
+                               threads if threads is not None else default_threads())
+    if st:
+        raise OracleError(f"oracle status {st}")
+    return out
+
+
+def find_extremes(image):
+    """(max_value, min_value, (max_x, max_y), (min_x, min_y))."""
+    a = np.ascontiguousarray(image)
+    H, W = a.shape
+    imax, imin = C.c_uint64(), C.c_uint64()
+    st = lib().tmo_find_extremes_index(_p(a), W, H, TYPE_CODES[a.dtype], C.byref(imax),
+                                       C.byref(imin))
+    if st:
+        raise OracleError(f"oracle status {st}")
+    flat = a.reshape(-1)
+    return (flat[imax.value], flat[imin.value], (imax.value % W, imax.value // W),
+            (imin.value % W, imin.value // W))
