@@ -106,3 +106,18 @@ def test_method_enum_matches_reference_order():
     assert [m.name for m in tm.MatchTemplateMethod] == [
         "SumOfSquaredErrors", "SumOfSquaredErrorsNormalized", "CrossCorrelation",
         "CrossCorrelationNormalized"]
+
+
+def test_cpp_mirror_raises_reference_panics(tmp_path):
+    import shutil
+    import subprocess
+    if not shutil.which("g++"):
+        pytest.skip("no C++ compiler")
+    exe = tmp_path / "hpp_panics"
+    lib_dir = _lib.LIB_PATH.parent
+    subprocess.run(["g++", "-std=c++17", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "cpp" / "hpp_panics.cpp"), "-L", str(lib_dir),
+                    "-limageproc_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == "ok"
