@@ -133,6 +133,8 @@ def lib() -> C.CDLL:
         C.c_void_p, u32, u32, C.c_void_p, u32, u32, C.c_void_p, u32, u32, C.c_int, C.c_int,
         C.c_int, C.c_void_p, C.c_void_p]
     L.ipb_match_template_device.restype = C.c_int
+    L.ipb_match_template_device_noalloc.argtypes = L.ipb_match_template_device.argtypes
+    L.ipb_match_template_device_noalloc.restype = C.c_int
     for suf, (ct, _) in EXTREMES_TYPES.items():
         f = getattr(L, f"ipb_find_extremes_{suf}")
         f.argtypes = [C.c_void_p, u32, u32, C.POINTER(EXTREMES_STRUCTS[suf])]

@@ -325,6 +325,9 @@ ipb_status extremes_device(const T* d_image, uint32_t W, uint32_t H, R* out, voi
 }
 
 }  // namespace
+
+int report_error(int st, const char* msg) { return fail(static_cast<ipb_status>(st), msg); }
+
 }  // namespace ipb
 
 using namespace ipb;

@@ -58,6 +58,9 @@ inline void timer_end(KernelTimer* t, cudaStream_t s) {
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Records `msg` as the calling thread's ipb_last_error_message and returns st.
+int report_error(int st, const char* msg);
+
 // ---- template preparation (tm_prep.cu) ----------------------------------
 // Byte planes of the template-side operands, each h rows of `pitch` bytes,
 // zero beyond w, followed by the u64 template constant TSS.

@@ -162,6 +162,27 @@ ipb_status ipb_match_template_device(
     int mask_is_binary, int method, int precision, float *d_out,
     void *stream);
 
+/* ipb_match_template_device without any memory allocation. No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc (a plug-in
+ * inside an application that owns the device-memory budget, a latency-critical
+ * loop where cudaMalloc/cudaFree would stall or synchronise the device, code
+ * that must not hit an out-of-memory failure after start-up). Same arguments
+ * and results as ipb_match_template_device; the caller still passes inputs and
+ * outputs. Its scratch memory is a fixed 16 MiB array inside the library,
+ * which every GPU that loads the library holds until the process exits;
+ * problems needing more (the u64 integral image of an unmasked SSE or
+ * normalised match takes (W+1)(H+1)*8 bytes, so images up to about 2.09
+ * megapixels) fail with IPB_ERR_INVALID_ARGUMENT and a message naming the
+ * size. The first call on each device looks up the array's device address
+ * (make it before any stream capture). All calls share the array: calls that
+ * overlap on the GPU race on it and must be ordered by the caller. */
+ipb_status ipb_match_template_device_noalloc(
+    const uint8_t *d_image, uint32_t image_width, uint32_t image_height,
+    const uint8_t *d_templ, uint32_t template_width, uint32_t template_height,
+    const uint8_t *d_mask, uint32_t mask_width, uint32_t mask_height,
+    int mask_is_binary, int method, int precision, float *d_out,
+    void *stream);
+
 /* ---- find_extremes -------------------------------------------------------- */
 
 /* Extremes<T> (src/template_matching.rs:463-475), field order kept. */
