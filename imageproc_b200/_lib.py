@@ -118,6 +118,8 @@ def lib() -> C.CDLL:
     L.ipb_version.restype = C.c_char_p
     L.ipb_set_precision.argtypes = [C.c_int]
     L.ipb_get_precision.restype = C.c_int
+    L.ipb_set_path.argtypes = [C.c_int]
+    L.ipb_get_path.restype = C.c_int
     L.ipb_launch_count.restype = C.c_uint64
     L.ipb_profile_enable.argtypes = [C.c_int]
     L.ipb_profile_collect.argtypes = [C.POINTER(KernelStats), C.c_int]

@@ -90,7 +90,7 @@ void note_timed(KernelTimer* t, double macs, double bytes) {
 const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
-      "template_sum_f32", "reference_f32", "find_extremes"};
+      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -111,6 +111,17 @@ int precision_from_env() {
   return IPB_PRECISION_EXACT_FP64;
 }
 std::atomic<int> g_precision{precision_from_env()};
+
+// Kernel family for exact matches: 0 = choose (tensor cores where the shape
+// allows), 1 = CUDA cores only, 2 = tensor cores wherever supported.
+int path_from_env() {
+  const char* v = std::getenv("IPB_PATH");
+  if (!v) return 0;
+  if (!std::strcmp(v, "1") || !std::strcmp(v, "cuda_core")) return 1;
+  if (!std::strcmp(v, "2") || !std::strcmp(v, "tensor")) return 2;
+  return 0;
+}
+std::atomic<int> g_path{path_from_env()};
 
 ipb_status fail(ipb_status st, const std::string& msg) {
   g_last_error = msg;
@@ -141,7 +152,8 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;  // last use of any scratch buffer below
   DevBuf scratch, ext_scratch, ext_result, img, tpl, mask, out;
-  void* pinned = nullptr;  // small pinned host block for reduction results
+  void* pinned = nullptr;  // small pinned host block: reduction results, error words
+  bool umma_pending = false;  // a tensor-core error word is on its way to pinned + 128
   ~Context() {
     if (device < 0) return;
     cudaSetDevice(device);
@@ -225,13 +237,26 @@ ipb_status run_match(Context* c, const MatchArgs& a) {
     return IPB_OK;
   }
   const bool ref = a.precision == IPB_PRECISION_REFERENCE_F32;
-  const size_t need = ref ? reference_scratch_bytes(a) : exact_cc_scratch_bytes(a);
+  const bool tensor = !ref && g_path.load() != 1 && umma_supported(a);
+  const size_t need = ref ? reference_scratch_bytes(a) : tensor ? umma_scratch_bytes(a) : exact_cc_scratch_bytes(a);
   ipb_status st = ensure(c, c->scratch, need);
   if (st) return st;
   IPB_CUDA(cudaStreamWaitEvent(a.stream, c->last, 0), "cudaStreamWaitEvent");
   MatchArgs la = a;
   la.timer = acquire_timer();
-  cudaError_t e = ref ? launch_reference(la, c->scratch.p) : launch_exact_cc(la, c->scratch.p);
+  // a wait that ran out in an earlier tensor-core launch on this context
+  if (c->umma_pending && cudaEventQuery(c->last) == cudaSuccess) {
+    c->umma_pending = false;
+    if (*reinterpret_cast<volatile unsigned int*>(static_cast<uint8_t*>(c->pinned) + 128))
+      return fail(IPB_ERR_TIMEOUT, "a tensor-core template-matching kernel timed out waiting on its pipeline");
+  }
+  cudaError_t e = ref ? launch_reference(la, c->scratch.p)
+                      : tensor ? launch_umma(la, c->scratch.p) : launch_exact_cc(la, c->scratch.p);
+  if (e == cudaSuccess && tensor) {
+    e = cudaMemcpyAsync(static_cast<uint8_t*>(c->pinned) + 128, umma_error_word(c->scratch.p, a),
+                        sizeof(unsigned int), cudaMemcpyDeviceToHost, a.stream);
+    c->umma_pending = true;
+  }
   if (la.timer) {
     const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
     note_timed(la.timer, Wo * Ho * tp,
@@ -269,6 +294,11 @@ ipb_status host_match(const uint8_t* image, uint32_t W, uint32_t H, const uint8_
   IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy scores");
   IPB_CUDA(cudaEventRecord(c->last, c->stream), "cudaEventRecord");
   IPB_CUDA(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  if (c->umma_pending) {
+    c->umma_pending = false;
+    if (*reinterpret_cast<volatile unsigned int*>(static_cast<uint8_t*>(c->pinned) + 128))
+      return fail(IPB_ERR_TIMEOUT, "a tensor-core template-matching kernel timed out waiting on its pipeline");
+  }
   return IPB_OK;
 }
 
@@ -371,6 +401,14 @@ IPB_API ipb_status ipb_set_precision(int precision) {
 }
 
 IPB_API int ipb_get_precision(void) { return g_precision.load(); }
+
+IPB_API ipb_status ipb_set_path(int path) {
+  if (path < 0 || path > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown kernel path");
+  g_path.store(path);
+  return IPB_OK;
+}
+
+IPB_API int ipb_get_path(void) { return g_path.load(); }
 
 IPB_API ipb_status ipb_match_template(const uint8_t* image, uint32_t W, uint32_t H, const uint8_t* tpl,
                                       uint32_t w, uint32_t h, int method, float* out) {

@@ -19,6 +19,7 @@ enum KernelId : int {
   kKernelTemplateSumF32,
   kKernelReference,
   kKernelExtremes,
+  kKernelUmma,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -85,6 +86,12 @@ cudaError_t launch_integral(const uint8_t* img, uint32_t W, uint32_t H,
 // ---- CUDA-core exact kernel (tm_exact_cc.cu) ------------------------------
 size_t exact_cc_scratch_bytes(const MatchArgs& a);
 cudaError_t launch_exact_cc(const MatchArgs& a, void* scratch);
+
+// ---- tensor-core exact kernel (tm_umma.cu) ---------------------------------
+bool umma_supported(const MatchArgs& a);
+size_t umma_scratch_bytes(const MatchArgs& a);
+cudaError_t launch_umma(const MatchArgs& a, void* scratch);
+unsigned int* umma_error_word(void* scratch, const MatchArgs& a);
 
 // ---- reference-order f32 kernel (tm_reference.cu) -------------------------
 size_t reference_scratch_bytes(const MatchArgs& a);

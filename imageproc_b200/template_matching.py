@@ -29,7 +29,7 @@ __all__ = [
     "MatchTemplateMethod", "Extremes", "Panic", "Precision",
     "match_template", "match_template_parallel",
     "match_template_with_mask", "match_template_with_mask_parallel",
-    "find_extremes", "set_precision", "get_precision",
+    "find_extremes", "set_precision", "get_precision", "Path", "set_path", "get_path",
 ]
 
 
@@ -67,6 +67,22 @@ def set_precision(precision: Precision | int) -> None:
 
 def get_precision() -> Precision:
     return Precision(_lib.lib().ipb_get_precision())
+
+
+class Path(enum.IntEnum):
+    """Kernel family of the exact precisions (identical results)."""
+
+    Auto = 0
+    CudaCores = 1
+    TensorCores = 2
+
+
+def set_path(path: Path | int) -> None:
+    check(_lib.lib().ipb_set_path(int(path)))
+
+
+def get_path() -> Path:
+    return Path(_lib.lib().ipb_get_path())
 
 
 def _gray(img: np.ndarray, what: str) -> np.ndarray:

@@ -90,6 +90,15 @@ const char *ipb_version(void);
 ipb_status ipb_set_precision(int precision);
 int ipb_get_precision(void);
 
+/* Kernel family of the exact precisions (no counterpart in the reference):
+ * 0 = automatic (tcgen05 tensor cores where the template shape allows, else
+ * CUDA cores), 1 = CUDA cores only, 2 = tensor cores wherever supported.
+ * Results are identical; the switch exists for testing and measurement.
+ * Initial value from the environment variable IPB_PATH (0/1/2 or
+ * auto/cuda_core/tensor). */
+ipb_status ipb_set_path(int path);
+int ipb_get_path(void);
+
 /* ---- tracing -------------------------------------------------------------
  * No counterpart in the reference (which has no instrumentation); used by the
  * benchmark and the profiling notes. */
