@@ -153,12 +153,15 @@ struct Context {
   cudaEvent_t last = nullptr;  // last use of any scratch buffer below
   DevBuf scratch, ext_scratch, ext_result, img, tpl, mask, out;
   void* pinned = nullptr;  // small pinned host block: reduction results, error words
-  bool umma_pending = false;  // a tensor-core error word is on its way to pinned + 128
+  DevBuf errw;                     // tensor-core error word (largest failing launch tag)
+  unsigned int tag = 0;            // tag of the last tensor-core launch
+  unsigned int tag_checked = 0;    // largest failing tag already reported
+  bool tensor_since_check = false;
   ~Context() {
     if (device < 0) return;
     cudaSetDevice(device);
     if (last) cudaEventSynchronize(last);
-    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out})
+    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw})
       if (b->p) cudaFree(b->p);
     if (pinned) cudaFreeHost(pinned);
     if (last) cudaEventDestroy(last);
@@ -228,6 +231,28 @@ bool host_mask_is_binary(const uint8_t* m, size_t n) {
   return true;
 }
 
+// Synchronises the stream and reports a tensor-core wait that ran out in any
+// launch of this context since the last check (the error word holds the
+// largest failing launch tag; tags only grow).
+ipb_status finish_sync(Context* c, cudaStream_t s) {
+  const bool check = c->tensor_since_check && c->errw.p;
+  if (check)
+    IPB_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(c->pinned) + 128, c->errw.p, sizeof(unsigned int),
+                             cudaMemcpyDeviceToHost, s),
+             "copy error word");
+  IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
+  IPB_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  if (check) {
+    c->tensor_since_check = false;
+    const unsigned int failed = *reinterpret_cast<volatile unsigned int*>(static_cast<uint8_t*>(c->pinned) + 128);
+    if (failed > c->tag_checked) {
+      c->tag_checked = failed;
+      return fail(IPB_ERR_TIMEOUT, "a tensor-core template-matching kernel timed out waiting on its pipeline");
+    }
+  }
+  return IPB_OK;
+}
+
 // Enqueue one matching problem on a.stream.
 ipb_status run_match(Context* c, const MatchArgs& a) {
   const size_t out_bytes = (size_t)(a.W - a.w + 1) * (a.H - a.h + 1) * sizeof(float);
@@ -238,24 +263,23 @@ ipb_status run_match(Context* c, const MatchArgs& a) {
   }
   const bool ref = a.precision == IPB_PRECISION_REFERENCE_F32;
   const bool tensor = !ref && g_path.load() != 1 && umma_supported(a);
-  const size_t need = ref ? reference_scratch_bytes(a) : tensor ? umma_scratch_bytes(a) : exact_cc_scratch_bytes(a);
-  ipb_status st = ensure(c, c->scratch, need);
-  if (st) return st;
+  ipb_status st;
+  if (tensor) {
+    if ((st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
+  } else {
+    const size_t need = ref ? reference_scratch_bytes(a) : exact_cc_scratch_bytes(a);
+    if ((st = ensure(c, c->scratch, need))) return st;
+  }
   IPB_CUDA(cudaStreamWaitEvent(a.stream, c->last, 0), "cudaStreamWaitEvent");
   MatchArgs la = a;
   la.timer = acquire_timer();
-  // a wait that ran out in an earlier tensor-core launch on this context
-  if (c->umma_pending && cudaEventQuery(c->last) == cudaSuccess) {
-    c->umma_pending = false;
-    if (*reinterpret_cast<volatile unsigned int*>(static_cast<uint8_t*>(c->pinned) + 128))
-      return fail(IPB_ERR_TIMEOUT, "a tensor-core template-matching kernel timed out waiting on its pipeline");
-  }
-  cudaError_t e = ref ? launch_reference(la, c->scratch.p)
-                      : tensor ? launch_umma(la, c->scratch.p) : launch_exact_cc(la, c->scratch.p);
-  if (e == cudaSuccess && tensor) {
-    e = cudaMemcpyAsync(static_cast<uint8_t*>(c->pinned) + 128, umma_error_word(c->scratch.p, a),
-                        sizeof(unsigned int), cudaMemcpyDeviceToHost, a.stream);
-    c->umma_pending = true;
+  cudaError_t e;
+  if (tensor) {
+    c->tag += 1;
+    c->tensor_since_check = true;
+    e = launch_umma(la, static_cast<unsigned int*>(c->errw.p), c->tag);
+  } else {
+    e = ref ? launch_reference(la, c->scratch.p) : launch_exact_cc(la, c->scratch.p);
   }
   if (la.timer) {
     const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
@@ -292,14 +316,7 @@ ipb_status host_match(const uint8_t* image, uint32_t W, uint32_t H, const uint8_
               static_cast<float*>(c->out.p), c->stream};
   if ((st = run_match(c, a))) return st;
   IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy scores");
-  IPB_CUDA(cudaEventRecord(c->last, c->stream), "cudaEventRecord");
-  IPB_CUDA(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
-  if (c->umma_pending) {
-    c->umma_pending = false;
-    if (*reinterpret_cast<volatile unsigned int*>(static_cast<uint8_t*>(c->pinned) + 128))
-      return fail(IPB_ERR_TIMEOUT, "a tensor-core template-matching kernel timed out waiting on its pipeline");
-  }
-  return IPB_OK;
+  return finish_sync(c, c->stream);
 }
 
 template <typename T, typename R>
@@ -317,8 +334,7 @@ ipb_status extremes_common(Context* c, const T* d, uint32_t W, uint32_t H, R* ou
   if (e != cudaSuccess) return cuda_fail(e, "find_extremes launch");
   IPB_CUDA(cudaMemcpyAsync(c->pinned, res, sizeof(ExtremesResult<DT>), cudaMemcpyDeviceToHost, s),
            "copy extremes");
-  IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
-  IPB_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  if ((st = finish_sync(c, s))) return st;
   ExtremesResult<DT> r;
   std::memcpy(&r, c->pinned, sizeof(r));
   out->max_value = (T)r.max_value;

@@ -47,6 +47,23 @@ __device__ __forceinline__ float finish_score(int method, int precision, unsigne
   return n > 0.0f ? __fdiv_rn(s, n) : s;
 }
 
+// finish_score for callers whose X, Y and TSS are all below 2^31 (templates
+// of at most 33025 pixels): the integer score fits in 32 bits, and SSE's
+// Y + TSS - 2X is exact in wrapping u32 arithmetic because the true result
+// is below 2^32. Same roundings as finish_score.
+__device__ __forceinline__ float finish_score32(int method, int precision, uint32_t X, uint32_t Y,
+                                                uint32_t tss) {
+  const uint32_t score = method_is_sse(method) ? (Y + tss - 2u * X) : X;
+  if (!method_is_norm(method)) return __uint2float_rn(score);
+  if (precision == IPB_PRECISION_EXACT_FP64) {
+    const double n = __dsqrt_rn(__dmul_rn(__uint2double_rn(Y), __uint2double_rn(tss)));
+    return n > 0.0 ? __double2float_rn(__ddiv_rn(__uint2double_rn(score), n)) : __uint2float_rn(score);
+  }
+  const float s = __uint2float_rn(score);
+  const float n = __fsqrt_rn(__fmul_rn(__uint2float_rn(Y), __uint2float_rn(tss)));
+  return n > 0.0f ? __fdiv_rn(s, n) : s;
+}
+
 __device__ __forceinline__ uint32_t dp4a_u8(uint32_t a, uint32_t b, uint32_t c) {
   return __dp4a(a, b, c);
 }

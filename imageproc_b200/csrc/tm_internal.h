@@ -88,10 +88,12 @@ size_t exact_cc_scratch_bytes(const MatchArgs& a);
 cudaError_t launch_exact_cc(const MatchArgs& a, void* scratch);
 
 // ---- tensor-core exact kernel (tm_umma.cu) ---------------------------------
+// One launch, no scratch: the kernel prepares the template side itself. A
+// bounded wait that runs out stores `tag` into *err_word (atomicMax), so the
+// word (zeroed once at allocation) tells whether a launch with that tag or a
+// later one failed.
 bool umma_supported(const MatchArgs& a);
-size_t umma_scratch_bytes(const MatchArgs& a);
-cudaError_t launch_umma(const MatchArgs& a, void* scratch);
-unsigned int* umma_error_word(void* scratch, const MatchArgs& a);
+cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag);
 
 // ---- reference-order f32 kernel (tm_reference.cu) -------------------------
 size_t reference_scratch_bytes(const MatchArgs& a);

@@ -58,6 +58,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
   return true;
 }
 
+// Same, for warps that are not on the critical path: between polls the warp
+// sleeps, leaving its scheduler's issue slots to the warps that are.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, unsigned long long deadline) {
+  uint32_t ns = 32;
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() > deadline) return false;
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+  return true;
+}
+
 // ---- proxy / tcgen05 ordering ------------------------------------------------
 // Generic-proxy writes to shared memory made visible to the async proxy (the
 // tensor core reads its B operand through it).
@@ -154,6 +166,52 @@ __device__ __forceinline__ void mma_i8_ts(uint32_t d_tmem, uint32_t a_tmem, uint
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
       "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// The same MMA executed by a whole converged warp: one elected lane issues
+// it, so warp-uniform operands stay in uniform registers (no per-operand
+// register-to-uniform moves in the issue loop). Always accumulates.
+__device__ __forceinline__ void mma_i8_ts_warp(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
+                                               uint32_t idesc) {
+  asm volatile(
+      "{\n\t.reg .pred e, acc;\n\t"
+      "setp.ne.b32 acc, 1, 0;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, acc;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc)
+      : "memory");
+}
+
+// True in exactly one lane of a converged warp.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred = 0;
+  asm volatile(
+      "{\n\t.reg .pred e;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "selp.u32 %0, 1, 0, e;\n\t}"
+      : "=r"(pred));
+  return pred != 0;
+}
+
+// Commit by one elected lane of a converged warp.
+__device__ __forceinline__ void mma_commit_warp(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .pred e;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+        "=r"(v[15])
+      : "r"(taddr)
       : "memory");
 }
 

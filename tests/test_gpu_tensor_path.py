@@ -79,3 +79,39 @@ def test_tensor_path_blob_scene_all_methods_exact_f32():
         got = run(image, template, method, tm.Path.TensorCores, tm.Precision.ExactF32)
         exp = O.match_exact(image, template, method, None, precision=1)
         assert bits(got).tolist() == bits(exp).tolist()
+
+
+MASK_SHAPES = [s for s in SHAPES if s[1][1] <= 128]
+
+
+@pytest.mark.parametrize("shape", MASK_SHAPES, ids=lambda s: f"{s[0][0]}x{s[0][1]}_t{s[1][0]}x{s[1][1]}")
+def test_tensor_path_binary_mask_bit_exact(shape):
+    (H, W), (h, w) = shape
+    g = np.random.default_rng(H * 11 + w)
+    image = g.integers(0, 256, (H, W), dtype=np.uint8)
+    template = g.integers(0, 256, (h, w), dtype=np.uint8)
+    mask = (g.random((h, w)) < 0.8).astype(np.uint8)
+    tm.set_path(tm.Path.TensorCores)
+    tm.set_precision(tm.Precision.ExactFp64)
+    for method in M:
+        got = tm.match_template_with_mask(image, template, method, mask)
+        exp = O.match_exact(image, template, method, mask, precision=0)
+        bad = np.argwhere(bits(got) != bits(exp))
+        assert bad.size == 0, (method, bad[:5], got[tuple(bad[0])], exp[tuple(bad[0])])
+
+
+def test_tensor_path_binary_mask_extremes():
+    g = np.random.default_rng(5)
+    image = g.integers(0, 256, (200, 300), dtype=np.uint8)
+    template = g.integers(0, 256, (40, 48), dtype=np.uint8)
+    tm.set_path(tm.Path.TensorCores)
+    for mask in (np.zeros((40, 48), np.uint8), np.ones((40, 48), np.uint8)):
+        for method in M:
+            got = tm.match_template_with_mask(image, template, method, mask)
+            exp = O.match_exact(image, template, method, mask, precision=0)
+            assert bits(got).tolist() == bits(exp).tolist()
+    ones = np.ones((40, 48), np.uint8)
+    for method in M:
+        a = tm.match_template_with_mask(image, template, method, ones)
+        b = tm.match_template(image, template, method)
+        assert bits(a).tolist() == bits(b).tolist()
