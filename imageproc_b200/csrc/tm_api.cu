@@ -374,6 +374,17 @@ ipb_status extremes_device(const T* d_image, uint32_t W, uint32_t H, R* out, voi
 
 int report_error(int st, const char* msg) { return fail(static_cast<ipb_status>(st), msg); }
 
+int check_match_args(uint32_t W, uint32_t H, uint32_t w, uint32_t h, bool masked, uint32_t mw, uint32_t mh,
+                     int method) {
+  return check_match(W, H, w, h, masked, mw, mh, method);
+}
+
+void count_launches(unsigned long long n) { g_launches.fetch_add(n); }
+bool profiling_enabled() { return g_profiling.load(); }
+KernelTimer* acquire_kernel_timer() { return acquire_timer(); }
+void note_kernel_timed(KernelTimer* t, double macs, double bytes) { note_timed(t, macs, bytes); }
+int kernel_path() { return g_path.load(); }
+
 }  // namespace ipb
 
 using namespace ipb;

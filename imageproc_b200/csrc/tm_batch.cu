@@ -1,0 +1,409 @@
+// tm_batch.cu -- batches of (image, template[, mask]) pairs: one persistent
+// tensor-core launch per group of compatible pairs, CUDA graphs, autotuning.
+//
+// The reference matches one pair per call (src/template_matching.rs:78, :125)
+// and finds extremes in a second pass (:479-511). Here a batch is planned once:
+//   * every pair is checked with the reference's assertions, in order;
+//   * a kernel family is chosen per pair: tcgen05 tensor cores where the
+//     template shape allows, else the CUDA-core exact kernel (or the
+//     reference-order kernel for REFERENCE_F32); the autotuner can time both
+//     on the first pair of each shape class and keep the faster;
+//   * tensor-core pairs are grouped by tensor-memory row width and mask
+//     kind, and each group runs as ONE persistent launch over all its tiles
+//     with find_extremes fused into the epilogue;
+//   * the launch sequence is captured once in a CUDA graph and replayed.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "tm_common.cuh"
+#include "tm_internal.h"
+
+#define IPB_API extern "C" __attribute__((visibility("default")))
+
+struct ipb_batch_plan {
+  int device = -1;
+  int precision = 0;
+  std::vector<ipb::MatchArgs> args;  // per pair, device pointers
+  std::vector<ipb_extremes_f32*> ext_out;
+  std::vector<bool> tensor;
+  struct Group {
+    ipb::UmmaPlan plan;
+    std::vector<uint32_t> members;
+    std::vector<ipb::UmmaProblem> probs;
+    ipb::UmmaProblem* d_probs = nullptr;
+    uint32_t tiles = 0;
+  };
+  std::vector<Group> groups;
+  // fused extremes of tensor pairs: keys {min, max}, map widths, output records
+  unsigned long long* d_keys = nullptr;
+  uint32_t* d_widths = nullptr;
+  ipb_extremes_f32** d_outs = nullptr;
+  uint32_t nkeys = 0;
+  // CUDA-core pairs: scratch and extremes scratch
+  void* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void* d_ext_scratch = nullptr;
+  ipb::ExtremesResult<float>* d_ext_result = nullptr;
+  unsigned int* d_err = nullptr;
+  unsigned int tag = 0;
+  uint32_t kernels = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace ipb {
+namespace {
+
+// ---- autotuner -----------------------------------------------------------------
+// Shape class of a pair: (w, h, masked, normalised). The decision is cached
+// per process and, when IPB_TUNING_FILE names a file, persisted across runs
+// ("w h masked norm tensor" per line).
+struct TuneKey {
+  uint32_t w, h;
+  int masked, norm;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(w, h, masked, norm) < std::tie(o.w, o.h, o.masked, o.norm);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, bool> g_tune;
+bool g_tune_loaded = false;
+
+void tune_load_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* f = std::getenv("IPB_TUNING_FILE");
+  if (!f) return;
+  std::ifstream in(f);
+  TuneKey k;
+  int t;
+  while (in >> k.w >> k.h >> k.masked >> k.norm >> t) g_tune[k] = t != 0;
+}
+
+void tune_store_locked() {
+  const char* f = std::getenv("IPB_TUNING_FILE");
+  if (!f) return;
+  std::ofstream out(f);
+  for (auto& kv : g_tune)
+    out << kv.first.w << ' ' << kv.first.h << ' ' << kv.first.masked << ' ' << kv.first.norm << ' '
+        << (kv.second ? 1 : 0) << '\n';
+}
+
+// Cost model: tensor cores whenever the shape is supported (they win from
+// 16x8 templates up; below that the CUDA-core kernel takes the pair).
+bool model_prefers_tensor(const MatchArgs& a) { return umma_supported(a); }
+
+float time_launch(const MatchArgs& a, bool tensor, void* scratch, unsigned int* err) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(e0, a.stream);
+    if (tensor) launch_umma(a, err, 0);
+    else launch_exact_cc(a, scratch);
+    cudaEventRecord(e1, a.stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best;
+}
+
+bool choose_tensor(const MatchArgs& a, bool autotune, void* scratch, unsigned int* err) {
+  if (!umma_supported(a)) return false;
+  const int path = kernel_path();
+  if (path == 1) return false;
+  if (path == 2 || !autotune) return model_prefers_tensor(a);
+  const TuneKey k{a.w, a.h, a.mask ? 1 : 0, method_is_norm(a.method) ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(k);
+    if (it != g_tune.end()) return it->second;
+  }
+  const float tt = time_launch(a, true, scratch, err);
+  const float tc = time_launch(a, false, scratch, err);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[k] = tt <= tc;
+  tune_store_locked();
+  return tt <= tc;
+}
+
+ipb_status to_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return IPB_OK;
+  const std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  (void)cudaGetLastError();
+  return (ipb_status)report_error(e == cudaErrorMemoryAllocation ? IPB_ERR_OUT_OF_MEMORY : IPB_ERR_CUDA,
+                                  msg.c_str());
+}
+
+#define IPB_TRY(call, what)                           \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return to_status(e_, what); \
+  } while (0)
+
+void release(ipb_batch_plan* p) {
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  for (auto& g : p->groups)
+    if (g.d_probs) cudaFree(g.d_probs);
+  for (void* b : {(void*)p->d_keys, (void*)p->d_widths, (void*)p->d_outs, p->d_scratch, p->d_ext_scratch,
+                  (void*)p->d_ext_result, (void*)p->d_err})
+    if (b) cudaFree(b);
+}
+
+// Enqueue the plan's launch sequence (used once under stream capture, and
+// directly when profiling so each kernel can be timed).
+ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kernels) {
+  uint32_t k = 0;
+  if (p->nkeys) {
+    IPB_TRY(launch_extremes_keys_init(p->d_keys, p->nkeys, s), "extremes init");
+    ++k;
+  }
+  for (auto& g : p->groups) {
+    UmmaLaunch L{};
+    const uint32_t n = (uint32_t)g.probs.size();
+    if (n <= kInlineProblems)
+      for (uint32_t i = 0; i < n; ++i) L.inl[i] = g.probs[i];
+    L.probs = g.d_probs;
+    L.nprobs = n;
+    L.tiles = g.tiles;
+    L.err = p->d_err;
+    L.tag = p->tag;
+    KernelTimer* t = timed ? acquire_kernel_timer() : nullptr;
+    IPB_TRY(launch_umma_batch(g.plan, L, s, t), "tensor-core batch launch");
+    if (t) {
+      double macs = 0, bytes = 0;
+      for (uint32_t i : g.members) {
+        const MatchArgs& a = p->args[i];
+        const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
+        macs += Wo * Ho * tp;
+        bytes += (double)a.W * a.H + tp * (a.mask ? 2.0 : 1.0) + 4.0 * Wo * Ho;
+      }
+      note_kernel_timed(t, macs, bytes);
+    }
+    ++k;
+  }
+  for (size_t i = 0; i < p->args.size(); ++i) {
+    if (p->tensor[i]) continue;
+    MatchArgs a = p->args[i];
+    a.stream = s;
+    if (a.w == 0 || a.h == 0) {
+      IPB_TRY(cudaMemsetAsync(a.out, 0, (size_t)(a.W - a.w + 1) * (a.H - a.h + 1) * sizeof(float), s), "memset");
+    } else if (a.precision == IPB_PRECISION_REFERENCE_F32) {
+      IPB_TRY(launch_reference(a, p->d_scratch), "reference launch");
+      k += 2;
+    } else {
+      IPB_TRY(launch_exact_cc(a, p->d_scratch), "CUDA-core launch");
+      k += (!a.mask && a.method != IPB_CROSS_CORRELATION) ? 4 : 2;
+    }
+    if (p->ext_out[i]) {
+      IPB_TRY(launch_find_extremes<float>(a.out, (unsigned long long)(a.W - a.w + 1) * (a.H - a.h + 1),
+                                          p->d_ext_scratch, p->d_ext_result, s),
+              "find_extremes launch");
+      IPB_TRY(launch_extremes_to_struct(p->d_ext_result, a.W - a.w + 1, p->ext_out[i], s), "extremes record");
+      k += 2;
+    }
+  }
+  if (p->nkeys) {
+    IPB_TRY(launch_extremes_keys_finish(p->d_keys, p->d_widths, p->d_outs, p->nkeys, s), "extremes finish");
+    ++k;
+  }
+  if (kernels) *kernels = k;
+  return IPB_OK;
+}
+
+ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture, ipb_batch_plan** out) {
+  if (!out || (n && !pairs)) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (precision < 0 || precision > 2) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "unknown precision");
+  for (uint32_t i = 0; i < n; ++i) {
+    const ipb_pair& q = pairs[i];
+    const int st = check_match_args(q.image_width, q.image_height, q.template_width, q.template_height,
+                                     q.mask != nullptr, q.mask_width, q.mask_height, q.method);
+    if (st != IPB_OK) {
+      std::string msg = std::string("pair ") + std::to_string(i) + ": " + ipb_last_error_message();
+      return (ipb_status)report_error(st, msg.c_str());
+    }
+    if (!q.out || (!q.image && (size_t)q.image_width * q.image_height) ||
+        (!q.templ && (size_t)q.template_width * q.template_height))
+      return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, ("pair " + std::to_string(i) + ": null buffer").c_str());
+  }
+  auto* p = new ipb_batch_plan();
+  cudaGetDevice(&p->device);
+  p->precision = precision;
+  p->args.resize(n);
+  p->ext_out.resize(n);
+  p->tensor.assign(n, false);
+  size_t scratch = 256;
+  for (uint32_t i = 0; i < n; ++i) {
+    const ipb_pair& q = pairs[i];
+    MatchArgs a{q.image, q.image_width, q.image_height, q.templ, q.template_width, q.template_height,
+                q.mask, q.mask && q.mask_is_binary != 0, q.method, precision, q.out, nullptr};
+    p->args[i] = a;
+    p->ext_out[i] = q.extremes;
+    if (a.w && a.h)
+      scratch = std::max(scratch, precision == IPB_PRECISION_REFERENCE_F32 ? reference_scratch_bytes(a)
+                                                                           : exact_cc_scratch_bytes(a));
+  }
+  auto fail = [&](ipb_status st) {
+    release(p);
+    delete p;
+    return st;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&p->d_scratch, scratch)) != cudaSuccess) return fail(to_status(e, "cudaMalloc"));
+  p->scratch_bytes = scratch;
+  if ((e = cudaMalloc(&p->d_err, sizeof(unsigned int))) != cudaSuccess) return fail(to_status(e, "cudaMalloc"));
+  cudaMemset(p->d_err, 0, sizeof(unsigned int));
+  if ((e = cudaMalloc(&p->d_ext_scratch, extremes_scratch_bytes())) != cudaSuccess)
+    return fail(to_status(e, "cudaMalloc"));
+  cudaMemset(p->d_ext_scratch, 0, extremes_scratch_bytes());
+  if ((e = cudaMalloc(&p->d_ext_result, sizeof(ExtremesResult<float>))) != cudaSuccess)
+    return fail(to_status(e, "cudaMalloc"));
+
+  // kernel family per pair, then tensor groups keyed by (row width, masked)
+  const bool autotune = std::getenv("IPB_AUTOTUNE") && std::strcmp(std::getenv("IPB_AUTOTUNE"), "1") == 0;
+  std::map<uint32_t, std::vector<uint32_t>> by_key;
+  for (uint32_t i = 0; i < n; ++i) {
+    MatchArgs a = p->args[i];
+    if (!a.w || !a.h) continue;
+    a.stream = nullptr;
+    if (choose_tensor(a, autotune, p->d_scratch, p->d_err)) {
+      p->tensor[i] = true;
+      by_key[umma_group_key(a)].push_back(i);
+    }
+  }
+  std::vector<unsigned long long> keys_host;
+  std::vector<uint32_t> widths;
+  std::vector<ipb_extremes_f32*> outs;
+  // one key slot per tensor pair with an extremes record
+  std::vector<int> slot(n, -1);
+  for (uint32_t i = 0; i < n; ++i)
+    if (p->tensor[i] && p->ext_out[i]) {
+      slot[i] = (int)widths.size();
+      widths.push_back(p->args[i].W - p->args[i].w + 1);
+      outs.push_back(p->ext_out[i]);
+    }
+  p->nkeys = (uint32_t)widths.size();
+  if (p->nkeys) {
+    if ((e = cudaMalloc(&p->d_keys, sizeof(unsigned long long) * 2 * p->nkeys)) != cudaSuccess ||
+        (e = cudaMalloc(&p->d_widths, sizeof(uint32_t) * p->nkeys)) != cudaSuccess ||
+        (e = cudaMalloc(&p->d_outs, sizeof(void*) * p->nkeys)) != cudaSuccess)
+      return fail(to_status(e, "cudaMalloc"));
+    cudaMemcpy(p->d_widths, widths.data(), sizeof(uint32_t) * p->nkeys, cudaMemcpyHostToDevice);
+    cudaMemcpy(p->d_outs, outs.data(), sizeof(void*) * p->nkeys, cudaMemcpyHostToDevice);
+  }
+  for (auto& kv : by_key) {
+    ipb_batch_plan::Group g;
+    uint32_t hmax = 0;
+    for (uint32_t i : kv.second) hmax = std::max(hmax, p->args[i].h);
+    const MatchArgs& a0 = p->args[kv.second.front()];
+    uint32_t ks = 8;
+    while (ks * 4 < ((a0.w + 31) & ~31u)) ks *= 2;
+    if (!umma_plan_for(ks, a0.mask != nullptr, hmax, g.plan)) return fail((ipb_status)report_error(IPB_ERR_CUDA, "no tensor-core plan"));
+    g.members = kv.second;
+    uint32_t tiles = 0;
+    for (uint32_t i : g.members) {
+      UmmaProblem q = umma_problem(p->args[i], g.plan, tiles, slot[i] >= 0 ? p->d_keys + 2 * slot[i] : nullptr);
+      tiles += umma_problem_tiles(q, g.plan);
+      g.probs.push_back(q);
+    }
+    g.tiles = tiles;
+    if (g.probs.size() > kInlineProblems) {
+      if ((e = cudaMalloc(&g.d_probs, sizeof(UmmaProblem) * g.probs.size())) != cudaSuccess)
+        return fail(to_status(e, "cudaMalloc"));
+      cudaMemcpy(g.d_probs, g.probs.data(), sizeof(UmmaProblem) * g.probs.size(), cudaMemcpyHostToDevice);
+    }
+    p->groups.push_back(std::move(g));
+  }
+  if ((e = umma_prepare_kernels()) != cudaSuccess) return fail(to_status(e, "kernel attributes"));
+  uint32_t kernels = 0;
+  if (capture) {
+    // capture the launch sequence once
+    cudaStream_t cs;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess)
+      return fail(to_status(e, "stream"));
+    ipb_status st = IPB_OK;
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      st = enqueue(p, cs, false, &kernels);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+      if (st == IPB_OK && e2 == cudaSuccess) {
+        p->graph = graph;
+        e = cudaGraphInstantiate(&p->exec, graph, 0);
+      } else if (e2 != cudaSuccess) {
+        e = e2;
+      }
+    }
+    cudaStreamDestroy(cs);
+    if (st != IPB_OK) return fail(st);
+    if (e != cudaSuccess) return fail(to_status(e, "graph capture"));
+    p->kernels = kernels;
+  }
+  *out = p;
+  return IPB_OK;
+}
+
+}  // namespace
+}  // namespace ipb
+
+using namespace ipb;
+
+IPB_API ipb_status ipb_batch_plan_create(const ipb_pair* pairs, uint32_t n, int precision, ipb_batch_plan** plan) {
+  return create(pairs, n, precision, /*capture=*/true, plan);
+}
+
+IPB_API ipb_status ipb_batch_plan_launch(ipb_batch_plan* plan, void* stream) {
+  if (!plan) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (profiling_enabled()) return enqueue(plan, s, true, nullptr);  // timed kernels, no graph
+  cudaError_t e = cudaGraphLaunch(plan->exec, s);
+  if (e != cudaSuccess) return to_status(e, "cudaGraphLaunch");
+  count_launches(plan->kernels);
+  return IPB_OK;
+}
+
+IPB_API ipb_status ipb_batch_plan_info(const ipb_batch_plan* plan, uint32_t* kernels, uint32_t* tensor_pairs) {
+  if (!plan) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null plan");
+  if (kernels) *kernels = plan->kernels;
+  if (tensor_pairs) *tensor_pairs = (uint32_t)std::count(plan->tensor.begin(), plan->tensor.end(), true);
+  return IPB_OK;
+}
+
+IPB_API ipb_status ipb_batch_plan_destroy(ipb_batch_plan* plan) {
+  if (!plan) return IPB_OK;
+  cudaDeviceSynchronize();
+  release(plan);
+  delete plan;
+  return IPB_OK;
+}
+
+IPB_API ipb_status ipb_match_template_batch_device(const ipb_pair* pairs, uint32_t n, int precision,
+                                                   void* stream) {
+  ipb_batch_plan* p = nullptr;
+  ipb_status st = create(pairs, n, precision, /*capture=*/false, &p);
+  if (st != IPB_OK) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st = enqueue(p, s, profiling_enabled(), nullptr);
+  // the plan's descriptors and scratch must outlive the enqueued work
+  const cudaError_t e = cudaStreamSynchronize(s);
+  release(p);
+  delete p;
+  if (st != IPB_OK) return st;
+  return to_status(e, "cudaStreamSynchronize");
+}

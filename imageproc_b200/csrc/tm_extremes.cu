@@ -178,6 +178,28 @@ cudaError_t launch_find_extremes(const T* d, unsigned long long n, void* scratch
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void extremes_result_to_struct_kernel(const ExtremesResult<float>* r, uint32_t width,
+                                                 ipb_extremes_f32* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  ipb_extremes_f32 e;
+  e.max_value = r->max_value;
+  e.min_value = r->min_value;
+  e.max_value_location_x = (uint32_t)(r->max_index % width);
+  e.max_value_location_y = (uint32_t)(r->max_index / width);
+  e.min_value_location_x = (uint32_t)(r->min_index % width);
+  e.min_value_location_y = (uint32_t)(r->min_index / width);
+  *out = e;
+}
+}  // namespace
+
+cudaError_t launch_extremes_to_struct(const ExtremesResult<float>* r, uint32_t width, ipb_extremes_f32* out,
+                                      cudaStream_t s) {
+  extremes_result_to_struct_kernel<<<1, 32, 0, s>>>(r, width, out);
+  count_launch(kKernelExtremes);
+  return cudaGetLastError();
+}
+
 #define IPB_INSTANTIATE_EXTREMES(T)                                                            \
   template cudaError_t launch_find_extremes<T>(const T*, unsigned long long, void*,            \
                                                ExtremesResult<T>*, cudaStream_t);

@@ -95,6 +95,53 @@ cudaError_t launch_exact_cc(const MatchArgs& a, void* scratch);
 bool umma_supported(const MatchArgs& a);
 cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag);
 
+// One problem of a tensor-core launch (device-side descriptor).
+struct UmmaProblem {
+  const uint8_t* img;
+  const uint8_t* tpl;
+  const uint8_t* mask;       // binary mask or null
+  float* out;
+  unsigned long long* ext;   // fused find_extremes keys {min, max} or null
+  uint32_t W, H, w, h;
+  uint32_t Wo, Ho, tiles_x, tile_begin;  // tile_begin: first global tile of the problem
+  uint32_t kmma, zrows, rows_max, load_mode;
+  int method, precision;
+};
+
+constexpr uint32_t kInlineProblems = 8;  // problems passed in the kernel parameters
+
+struct UmmaLaunch {
+  UmmaProblem inl[kInlineProblems];
+  const UmmaProblem* probs;  // device array when nprobs > kInlineProblems
+  uint32_t nprobs, tiles;
+  uint32_t NT, rps, imgp, plane_bytes, nbuf;
+  uint32_t z_off, img_off, rs_off;
+  unsigned int* err;
+  unsigned int tag;
+};
+
+// Launch-wide plan of a group of problems sharing (tensor-memory row width,
+// masked): tile height, pipeline depth and shared-memory carve.
+struct UmmaPlan {
+  uint32_t ks;
+  bool masked;
+  uint32_t NT, rps, imgp, plane_bytes, nbuf, z_off, img_off, rs_off, smem;
+};
+
+uint32_t umma_group_key(const MatchArgs& a);
+// Sets every tensor-core kernel's shared-memory limit (outside stream capture).
+cudaError_t umma_prepare_kernels();
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl);
+UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
+                         unsigned long long* ext_keys);
+uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl);
+// Fills the plan fields of L and launches (L.inl / L.probs, nprobs, tiles,
+// err, tag set by the caller).
+cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t stream, KernelTimer* timer);
+cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s);
+cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const uint32_t* widths,
+                                        ipb_extremes_f32* const* outs, uint32_t n, cudaStream_t s);
+
 // ---- reference-order f32 kernel (tm_reference.cu) -------------------------
 size_t reference_scratch_bytes(const MatchArgs& a);
 cudaError_t launch_reference(const MatchArgs& a, void* scratch);
@@ -112,5 +159,18 @@ size_t extremes_scratch_bytes();
 template <typename T>
 cudaError_t launch_find_extremes(const T* d, unsigned long long n, void* scratch,
                                  ExtremesResult<T>* d_result, cudaStream_t s);
+// ExtremesResult<float> of a map of the given width -> ipb_extremes_f32 (device)
+cudaError_t launch_extremes_to_struct(const ExtremesResult<float>* r, uint32_t width, ipb_extremes_f32* out,
+                                      cudaStream_t s);
+
+// Validation shared by the single and batched entry points: the reference's
+// assertions in its order; returns the status and sets the thread's message.
+int check_match_args(uint32_t W, uint32_t H, uint32_t w, uint32_t h, bool masked, uint32_t mw, uint32_t mh,
+                     int method);
+void count_launches(unsigned long long n);
+bool profiling_enabled();
+KernelTimer* acquire_kernel_timer();
+void note_kernel_timed(KernelTimer* t, double macs, double bytes);
+int kernel_path();  // 0 auto, 1 CUDA cores, 2 tensor cores
 
 }  // namespace ipb

@@ -3,7 +3,9 @@
 //
 // Replaces the scalar walk of methods::*::score_at (src/template_matching.rs:
 // 219-376) for unmasked and binary-masked matches with templates up to
-// 256 x 128 pixels (128 x 128 masked).
+// 256 x 128 pixels (128 x 128 masked), for one problem or a batch of many
+// (image, template) pairs of uneven sizes in one persistent launch, with
+// find_extremes (:479-511) optionally fused into the epilogue.
 //
 // Formulation. A CTA owns a tile of 128 output columns (x0 + m, m = tensor-
 // memory lane) by NT output rows (y0 + n, n = tensor-memory column). For each
@@ -22,22 +24,25 @@
 // rows are 16 bytes apart: moving from r to r+1 moves B's start address by
 // -16 bytes. Only the 16-aligned band of n where B_r is non-zero is issued.
 //
-// A_r goes straight into tensor memory: eight builder warps form each lane's
-// K bytes from the staged image rows with byte_perm and store them with
-// tcgen05.st (the MMA reads A from tensor memory and only B from shared
-// memory). Unmasked, the same words give the lane's row sum of squares with
-// dp4a, from which the epilogue slides the window sum Y = sum I^2 over h rows,
-// so no integral image is needed. The kernel also builds Z and the template
-// constant TSS from the raw template (and mask) itself: a call is one launch.
+// A_r goes straight into tensor memory: sixteen builder warps (four per
+// tensor-memory lane quadrant) form each lane's K bytes from the staged image
+// rows with byte_perm and store them with tcgen05.st; the MMA reads A from
+// tensor memory and only B from shared memory. Unmasked, the same words give
+// the lane's row sum of squares with dp4a, from which the epilogue slides the
+// window sum Y = sum I^2 over h rows, so no integral image is needed. The
+// kernel builds Z and the template constant TSS from the raw template (and
+// mask) whenever a CTA moves to a tile of another problem.
 //
 // Pipeline: image tiles are double-buffered in shared memory and loaded with
 // cp.async while the previous tile is computed. Builders fill 3 stages of RPS
-// A rows; one thread issues the MMAs of a stage from a per-tile table once the
-// stage is full and commits it back to the builders; after the tile's last
-// stage it commits the accumulators to the epilogue (the builder warps), which
-// reads them with tcgen05.ld and writes the scores. Every wait is bounded
-// (2 s); a wait that runs out records the launch's tag in the error word and
-// the CTA leaves its loop, drains its MMAs and frees its tensor memory.
+// A rows; one warp runs the MMA issue loop on warp-uniform values and one
+// elected lane issues the MMAs of a stage once it is full, then commits it
+// back to the builders; after the tile's last stage it commits the
+// accumulators to the epilogue (the builder warps), which reads them with
+// tcgen05.ld, writes the scores and folds them into the problem's extremes.
+// Every wait is bounded (2 s); a wait that runs out records the launch's tag
+// in the error word and the CTA leaves its loop, drains its MMAs and frees its
+// tensor memory.
 #include "tm_common.cuh"
 #include "tm_internal.h"
 #include "tm_sm100.cuh"
@@ -52,35 +57,13 @@ constexpr int kBuilderWarps = 16;
 constexpr int kSubs = kBuilderWarps / 4;  // builder warps per tensor-memory lane quadrant
 constexpr int kBuilders = kBuilderWarps * 32;
 constexpr int kThreads = kBuilders + 32;
+constexpr int kWarps = kThreads / 32;
 constexpr int kStages = 3;
 constexpr uint32_t kMaxRps = 16;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr uint32_t kSmemHeader = 1024;
 constexpr uint32_t kMinSmem = 120 * 1024;  // keeps residency at one CTA per SM
-
-struct UmmaParams {
-  const uint8_t* img;
-  uint32_t W, H;
-  const uint8_t* tpl;   // raw template, w x h
-  const uint8_t* mask;  // raw binary mask or null
-  uint32_t w, h;
-  uint32_t kmma;      // K of the MMAs: w rounded up to 32
-  uint32_t NT;        // output rows per tile
-  uint32_t rps;       // image rows per pipeline stage
-  uint32_t imgp;      // staged image row pitch (bytes)
-  uint32_t rows_max;  // NT + h - 1
-  uint32_t zrows;     // rows of a reversed-template buffer: h + 32
-  uint32_t zplane;    // bytes of one reversed-template buffer
-  uint32_t tab_off, z_off, img_off, rs_off;  // shared-memory carve
-  uint32_t plane_bytes;  // one staged image plane: rows_max * imgp
-  uint32_t nbuf;         // staged image buffers (1 or 2)
-  uint32_t Wo, Ho, tiles_x, tiles;
-  int method, precision, load_mode;  // load_mode: 2 = cp.async 16 B, 1 = 4 B, 0 = plain loads
-  float* out;
-  unsigned int* err;
-  unsigned int tag;
-};
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
@@ -91,39 +74,47 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, uint32_
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Stage image rows [y0, y0 + nrows) x columns [x0, x0 + imgp) of plane 0,
-// zero past the right edge. Asynchronous unless load_mode == 0.
-__device__ void issue_tile_load(const UmmaParams& p, uint8_t* dst_plane, uint32_t tile) {
-  const uint32_t x0 = (tile % p.tiles_x) * kM;
-  const uint32_t y0 = (tile / p.tiles_x) * p.NT;
-  const uint32_t nrows = min(p.rows_max, p.H - y0);
-  const uint8_t* src = p.img + (size_t)y0 * p.W;
-  if (p.load_mode == 2) {
-    const uint32_t chunks = p.imgp / 16;
+// problem index of a global tile, advancing monotonically from `pi`
+__device__ __forceinline__ uint32_t find_problem(const UmmaLaunch& L, const UmmaProblem* P, uint32_t pi,
+                                                 uint32_t tile) {
+  while (pi + 1 < L.nprobs && tile >= P[pi + 1].tile_begin) ++pi;
+  return pi;
+}
+
+// Stage image rows [y0, y0 + nrows) x columns [x0, x0 + imgp) of plane 0 for
+// the problem's local tile, zero past the right edge. Asynchronous unless the
+// image rows are not 4-byte aligned.
+__device__ void issue_tile_load(const UmmaLaunch& L, const UmmaProblem q, uint8_t* dst_plane, uint32_t lt) {
+  const uint32_t x0 = (lt % q.tiles_x) * kM;
+  const uint32_t y0 = (lt / q.tiles_x) * L.NT;
+  const uint32_t nrows = min(q.rows_max, q.H - y0);
+  const uint8_t* src = q.img + (size_t)y0 * q.W;
+  if (q.load_mode == 2) {
+    const uint32_t chunks = L.imgp / 16;
     for (uint32_t idx = threadIdx.x; idx < nrows * chunks; idx += kThreads) {
       const uint32_t r = idx / chunks, c = (idx % chunks) * 16, gx = x0 + c;
-      const uint32_t avail = gx < p.W ? min(16u, p.W - gx) : 0u;
-      const uint8_t* g = src + (size_t)r * p.W + (avail ? gx : 0u);
-      cp_async16(smem_u32(dst_plane + r * p.imgp + c), g, avail);
+      const uint32_t avail = gx < q.W ? min(16u, q.W - gx) : 0u;
+      const uint8_t* g = src + (size_t)r * q.W + (avail ? gx : 0u);
+      cp_async16(smem_u32(dst_plane + r * L.imgp + c), g, avail);
     }
-  } else if (p.load_mode == 1) {
-    const uint32_t words = p.imgp / 4;
+  } else if (q.load_mode == 1) {
+    const uint32_t words = L.imgp / 4;
     for (uint32_t idx = threadIdx.x; idx < nrows * words; idx += kThreads) {
       const uint32_t r = idx / words, c = (idx % words) * 4, gx = x0 + c;
-      const uint32_t avail = gx < p.W ? min(4u, p.W - gx) : 0u;
-      const uint8_t* g = src + (size_t)r * p.W + (avail ? gx : 0u);
-      cp_async4(smem_u32(dst_plane + r * p.imgp + c), g, avail);
+      const uint32_t avail = gx < q.W ? min(4u, q.W - gx) : 0u;
+      const uint8_t* g = src + (size_t)r * q.W + (avail ? gx : 0u);
+      cp_async4(smem_u32(dst_plane + r * L.imgp + c), g, avail);
     }
   } else {
-    const uint32_t words = p.imgp / 4;
+    const uint32_t words = L.imgp / 4;
     for (uint32_t idx = threadIdx.x; idx < nrows * words; idx += kThreads) {
       const uint32_t r = idx / words, c = (idx % words) * 4, gx = x0 + c;
-      const uint8_t* row = src + (size_t)r * p.W;
+      const uint8_t* row = src + (size_t)r * q.W;
       uint32_t v = 0;
 #pragma unroll
       for (int k = 0; k < 4; ++k)
-        if (gx + k < p.W) v |= (uint32_t)__ldg(row + gx + k) << (8 * k);
-      *reinterpret_cast<uint32_t*>(dst_plane + r * p.imgp + c) = v;
+        if (gx + k < q.W) v |= (uint32_t)__ldg(row + gx + k) << (8 * k);
+      *reinterpret_cast<uint32_t*>(dst_plane + r * L.imgp + c) = v;
     }
   }
   cp_async_commit();
@@ -167,10 +158,17 @@ __device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t
   return rs;
 }
 
+// Order-preserving key of a finite f32 score (larger value -> larger key).
+__device__ __forceinline__ uint32_t order_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
 template <int KS, bool MASKED>
-__global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParams p) {
+__global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_constant__ UmmaLaunch L) {
   constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, low, high byte of I^2)
   constexpr int NCORR = MASKED ? 3 : 1;  // correlations / accumulators
+  constexpr int NZ = MASKED ? 2 : 1;     // reversed-template buffers
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kStages;
@@ -178,10 +176,11 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
   uint64_t* drain = dfull + 1;
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + 128);
   volatile int* s_err = reinterpret_cast<volatile int*>(smem + 132);
-  unsigned long long* s_tss = reinterpret_cast<unsigned long long*>(smem + 136);
-  uint8_t* zbuf = smem + p.z_off;
-  uint8_t* s_img = smem + p.img_off;
-  uint32_t* s_rs = reinterpret_cast<uint32_t*>(smem + p.rs_off);
+  unsigned long long* s_part = reinterpret_cast<unsigned long long*>(smem + 256);  // kWarps partial sums
+  uint8_t* zbuf = smem + L.z_off;
+  uint8_t* s_img = smem + L.img_off;
+  uint32_t* s_rs = reinterpret_cast<uint32_t*>(smem + L.rs_off);
+  const UmmaProblem* P = L.nprobs <= kInlineProblems ? L.inl : L.probs;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool mma_warp = warp == kBuilderWarps;
@@ -194,91 +193,103 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
     mbar_init(dfull, 1);
     mbar_init(drain, 1);
     *s_err = 0;
-    *s_tss = 0ull;
     mbar_init_fence();
   }
   if (mma_warp) {
     tmem_alloc(s_tmem, kTmemCols);
     tmem_relinquish();
   }
+  uint32_t pi = 0;
   // first tile's rows start streaming in while the template side is prepared
-  if (blockIdx.x < p.tiles) issue_tile_load(p, s_img, blockIdx.x);
-  __syncthreads();  // s_tss initialised
-  // Z buffers, K-chunk-major: chunk c holds rows j = 0..zrows-1 of 16 bytes,
-  // row j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
-  //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m
-  {
-    constexpr int NZ = MASKED ? 2 : 1;
-    const uint32_t nchunks = p.kmma / 16;
-    for (uint32_t idx = threadIdx.x; idx < NZ * nchunks * p.zrows; idx += kThreads) {
-      const uint32_t zp = idx / (nchunks * p.zrows);
-      const uint32_t rem = idx % (nchunks * p.zrows);
-      const uint32_t c = rem / p.zrows, j = rem % p.zrows;
-      uint32_t wd[4] = {0u, 0u, 0u, 0u};
-      if (j >= 16 && j < p.h + 16) {
-        const size_t row = (size_t)(p.h - 1 - (j - 16)) * p.w;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const uint32_t dx = 16 * c + k;
-          if (dx < p.w) {
-            uint32_t v;
-            if constexpr (MASKED) {
-              const uint32_t mv = __ldg(p.mask + row + dx);
-              v = zp == 0 ? (uint32_t)__ldg(p.tpl + row + dx) * mv : mv;
-            } else {
-              v = __ldg(p.tpl + row + dx);
-            }
-            wd[k >> 2] |= (v & 0xFFu) << (8 * (k & 3));
-          }
-        }
-      }
-      *reinterpret_cast<uint4*>(zbuf + zp * p.zplane + (size_t)(c * p.zrows + j) * 16) =
-          make_uint4(wd[0], wd[1], wd[2], wd[3]);
-    }
-    // TSS = sum (T*m)^2 (m = 1 unmasked), exact in u64
-    unsigned long long t2 = 0;
-    for (uint32_t k = threadIdx.x; k < p.w * p.h; k += kThreads) {
-      uint32_t t = __ldg(p.tpl + k);
-      if constexpr (MASKED) t *= __ldg(p.mask + k);
-      t2 += (unsigned long long)t * t;
-    }
-    for (int o = 16; o > 0; o >>= 1) t2 += __shfl_down_sync(0xffffffffu, t2, o);
-    if (lane == 0 && t2) atomicAdd(s_tss, t2);
+  if (blockIdx.x < L.tiles) {
+    pi = find_problem(L, P, 0, blockIdx.x);
+    issue_tile_load(L, P[pi], s_img, blockIdx.x - P[pi].tile_begin);
   }
-  fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  const uint32_t a_col0 = NCORR * p.NT;
+  const uint32_t a_col0 = NCORR * L.NT;
   const uint32_t a_row_cols = NPL * KS;
-  const uint32_t tss = (uint32_t)*s_tss;  // < 2^31: at most 33025 template pixels
-  const uint64_t desc0 = smem_desc_noswizzle(smem_u32(zbuf), p.zrows * 16, 128);
   const uint32_t idesc0 = idesc_u8u8_s32(kM, 16) & ~(0x3Fu << 17);
-  const uint32_t ksteps = p.kmma / 32;
 
-  uint32_t g = 0;       // pipeline stage fills so far (same count in builders and the MMA thread)
-  uint32_t tcount = 0;  // tiles finished by this CTA
+  uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
+  uint32_t tcount = 0;       // tiles finished by this CTA
+  uint32_t zp_loaded = ~0u;  // problem whose Z buffers and TSS are in shared memory
+  uint32_t tss = 0;
   bool ok = true;
 
-  for (uint32_t tile = blockIdx.x; tile < p.tiles; tile += gridDim.x, ++tcount) {
+  for (uint32_t tile = blockIdx.x; tile < L.tiles; tile += gridDim.x, ++tcount) {
     __syncthreads();
     if (*s_err) break;
-    const uint32_t buf = p.nbuf == 2 ? (tcount & 1u) : 0u;
-    uint8_t* img_buf = s_img + buf * NPL * p.plane_bytes;
-    if (p.nbuf == 1 && tcount > 0) issue_tile_load(p, img_buf, tile);
-    const uint32_t x0 = (tile % p.tiles_x) * kM;
-    const uint32_t y0 = (tile / p.tiles_x) * p.NT;
-    const uint32_t nrows = min(p.rows_max, p.H - y0);
+    pi = find_problem(L, P, pi, tile);
+    // a register copy: the tcgen05/cp.async asm statements clobber memory,
+    // which would otherwise force every use to reload the field
+    const UmmaProblem q = P[pi];
+    const uint32_t lt = tile - q.tile_begin;
+    const uint32_t buf = L.nbuf == 2 ? (tcount & 1u) : 0u;
+    uint8_t* img_buf = s_img + buf * NPL * L.plane_bytes;
+    if (L.nbuf == 1 && tcount > 0) issue_tile_load(L, q, img_buf, lt);
+    const uint32_t x0 = (lt % q.tiles_x) * kM;
+    const uint32_t y0 = (lt / q.tiles_x) * L.NT;
+    const uint32_t nrows = min(q.rows_max, q.H - y0);
+    const uint32_t zplane = (q.kmma / 16) * q.zrows * 16;
+    if (pi != zp_loaded) {
+      // Z buffers, K-chunk-major: chunk c holds rows j = 0..zrows-1 of 16 bytes,
+      // row j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
+      //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m
+      const uint32_t nchunks = q.kmma / 16;
+      for (uint32_t idx = threadIdx.x; idx < NZ * nchunks * q.zrows; idx += kThreads) {
+        const uint32_t zp = idx / (nchunks * q.zrows);
+        const uint32_t rem = idx % (nchunks * q.zrows);
+        const uint32_t c = rem / q.zrows, j = rem % q.zrows;
+        uint32_t wd[4] = {0u, 0u, 0u, 0u};
+        if (j >= 16 && j < q.h + 16) {
+          const size_t row = (size_t)(q.h - 1 - (j - 16)) * q.w;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const uint32_t dx = 16 * c + k;
+            if (dx < q.w) {
+              uint32_t v;
+              if constexpr (MASKED) {
+                const uint32_t mv = __ldg(q.mask + row + dx);
+                v = zp == 0 ? (uint32_t)__ldg(q.tpl + row + dx) * mv : mv;
+              } else {
+                v = __ldg(q.tpl + row + dx);
+              }
+              wd[k >> 2] |= (v & 0xFFu) << (8 * (k & 3));
+            }
+          }
+        }
+        *reinterpret_cast<uint4*>(zbuf + zp * zplane + (size_t)(c * q.zrows + j) * 16) =
+            make_uint4(wd[0], wd[1], wd[2], wd[3]);
+      }
+      // TSS = sum (T*m)^2 (m = 1 unmasked), exact; per-warp partials in shared memory
+      unsigned long long t2 = 0;
+      for (uint32_t k = threadIdx.x; k < q.w * q.h; k += kThreads) {
+        uint32_t t = __ldg(q.tpl + k);
+        if constexpr (MASKED) t *= __ldg(q.mask + k);
+        t2 += (unsigned long long)t * t;
+      }
+      for (int o = 16; o > 0; o >>= 1) t2 += __shfl_down_sync(0xffffffffu, t2, o);
+      if (lane == 0) s_part[warp] = t2;
+      fence_proxy_async_smem();
+    }
     cp_async_wait_all();
     __syncthreads();
     if (*s_err) break;
+    if (pi != zp_loaded) {
+      unsigned long long t = 0;
+      for (int k = 0; k < kWarps; ++k) t += s_part[k];
+      tss = (uint32_t)t;  // < 2^31: at most 33025 template pixels
+      zp_loaded = pi;
+    }
     if constexpr (MASKED) {
       // byte planes of I^2 next to the staged image
-      const uint32_t words = nrows * p.imgp / 4;
+      const uint32_t words = nrows * L.imgp / 4;
       const uint32_t* i4 = reinterpret_cast<const uint32_t*>(img_buf);
-      uint32_t* lo4 = reinterpret_cast<uint32_t*>(img_buf + p.plane_bytes);
-      uint32_t* hi4 = reinterpret_cast<uint32_t*>(img_buf + 2 * p.plane_bytes);
+      uint32_t* lo4 = reinterpret_cast<uint32_t*>(img_buf + L.plane_bytes);
+      uint32_t* hi4 = reinterpret_cast<uint32_t*>(img_buf + 2 * L.plane_bytes);
       for (uint32_t idx = threadIdx.x; idx < words; idx += kThreads) {
         const uint32_t v = i4[idx];
         uint32_t lo = 0, hi = 0;
@@ -295,25 +306,26 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
       __syncthreads();
     }
     // the next tile's rows stream into the other buffer during this tile
-    if (p.nbuf == 2 && tile + gridDim.x < p.tiles)
-      issue_tile_load(p, s_img + (buf ^ 1u) * NPL * p.plane_bytes, tile + gridDim.x);
-    const uint32_t nst = (nrows + p.rps - 1) / p.rps;
+    if (L.nbuf == 2 && tile + gridDim.x < L.tiles) {
+      const uint32_t pn = find_problem(L, P, pi, tile + gridDim.x);
+      issue_tile_load(L, P[pn], s_img + (buf ^ 1u) * NPL * L.plane_bytes, tile + gridDim.x - P[pn].tile_begin);
+    }
+    const uint32_t nst = (nrows + L.rps - 1) / L.rps;
     const unsigned long long deadline = global_ns() + kWaitNs;
 
     if (!mma_warp) {
-      // builder warp: lane quadrant q of tensor memory, sub-group sub (4 per quadrant)
-      const uint32_t q = warp & 3, sub = warp >> 2;
-      const uint32_t m = q * 32 + lane;
-      const uint32_t lane_base = q * 32;
-      const uint32_t ncols = p.NT / kSubs;  // accumulator columns this warp zeroes and finishes
+      // builder warp: lane quadrant q4 of tensor memory, sub-group sub (kSubs per quadrant)
+      const uint32_t q4 = warp & 3, sub = warp >> 2;
+      const uint32_t m = q4 * 32 + lane;
+      const uint32_t lane_base = q4 * 32;
+      const uint32_t ncols = L.NT / kSubs;  // accumulator columns this warp zeroes and finishes
       const uint32_t c_begin = sub * ncols;
-      // zero this warp's share of the accumulators
       {
         const uint32_t zero16[16] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
         for (int c = 0; c < NCORR; ++c)
           for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
-            tmem_st16(tmem_addr(tmem, lane_base, c * p.NT + col), zero16);
+            tmem_st16(tmem_addr(tmem, lane_base, c * L.NT + col), zero16);
       }
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
@@ -322,17 +334,17 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
           break;
         }
         tc_fence_after();
-        const uint32_t r0 = st * p.rps, r_end = min(nrows, r0 + p.rps);
+        const uint32_t r0 = st * L.rps, r_end = min(nrows, r0 + L.rps);
         // rows r == sub (mod kSubs) of this stage
         for (uint32_t r = r0 + ((sub + kSubs - (r0 % kSubs)) % kSubs); r < r_end; r += kSubs) {
-          const uint32_t tcol = a_col0 + (s * p.rps + (r - r0)) * a_row_cols;
-          const uint8_t* row = img_buf + r * p.imgp;
+          const uint32_t tcol = a_col0 + (s * L.rps + (r - r0)) * a_row_cols;
+          const uint8_t* row = img_buf + r * L.imgp;
           if constexpr (MASKED) {
 #pragma unroll
             for (int pl = 0; pl < NPL; ++pl)
-              build_row<KS, false>(row + pl * p.plane_bytes, m, p.w, tmem_addr(tmem, lane_base, tcol + pl * KS));
+              build_row<KS, false>(row + pl * L.plane_bytes, m, q.w, tmem_addr(tmem, lane_base, tcol + pl * KS));
           } else {
-            s_rs[r * kM + m] = build_row<KS, true>(row, m, p.w, tmem_addr(tmem, lane_base, tcol));
+            s_rs[r * kM + m] = build_row<KS, true>(row, m, q.w, tmem_addr(tmem, lane_base, tcol));
           }
         }
         tmem_wait_st();
@@ -350,26 +362,27 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
         if constexpr (!MASKED) {
           uint32_t y4[4] = {0u, 0u, 0u, 0u};
           uint32_t r = c_begin;
-          for (; r + 4 <= c_begin + p.h; r += 4)
+          for (; r + 4 <= c_begin + q.h; r += 4)
 #pragma unroll
             for (int k = 0; k < 4; ++k) y4[k] += (r + k < nrows) ? s_rs[(r + k) * kM + m] : 0u;
-          for (; r < c_begin + p.h; ++r) y4[0] += r < nrows ? s_rs[r * kM + m] : 0u;
+          for (; r < c_begin + q.h; ++r) y4[0] += r < nrows ? s_rs[r * kM + m] : 0u;
           Y = y4[0] + y4[1] + y4[2] + y4[3];
         }
+        unsigned long long kmin = ~0ull, kmax = 0ull;
         for (uint32_t n0 = c_begin; n0 < c_begin + ncols; n0 += 16) {
           uint32_t vx[16];
           tmem_ld16(tmem_addr(tmem, lane_base, n0), vx);
           uint32_t vl[MASKED ? 16 : 1], vh[MASKED ? 16 : 1];
           uint32_t yv[16];
           if constexpr (MASKED) {
-            tmem_ld16(tmem_addr(tmem, lane_base, p.NT + n0), vl);
-            tmem_ld16(tmem_addr(tmem, lane_base, 2 * p.NT + n0), vh);
+            tmem_ld16(tmem_addr(tmem, lane_base, L.NT + n0), vl);
+            tmem_ld16(tmem_addr(tmem, lane_base, 2 * L.NT + n0), vh);
           } else {
             // window sums of the chunk: loads first, then the sliding chain
             uint32_t add[16], subv[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
-              const uint32_t ra = n0 + k + p.h, rb = n0 + k;
+              const uint32_t ra = n0 + k + q.h, rb = n0 + k;
               add[k] = ra < nrows ? s_rs[ra * kM + m] : 0u;
               subv[k] = rb < nrows ? s_rs[rb * kM + m] : 0u;
             }
@@ -387,21 +400,44 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
             uint32_t Yk;
             if constexpr (MASKED) Yk = vl[k] + (vh[k] << 8);
             else Yk = yv[k];
-            if (x < p.Wo && y < p.Ho)
-              p.out[(size_t)y * p.Wo + x] = finish_score32(p.method, p.precision, vx[k], Yk, tss);
+            if (x < q.Wo && y < q.Ho) {
+              const float f = finish_score32(q.method, q.precision, vx[k], Yk, tss);
+              const uint32_t lin = y * q.Wo + x;
+              q.out[(size_t)lin] = f;
+              if (q.ext) {
+                const unsigned long long key = (unsigned long long)order_key(f) << 32;
+                kmin = min(kmin, key | lin);
+                kmax = max(kmax, key | (0xFFFFFFFFu - lin));
+              }
+            }
+          }
+        }
+        if (q.ext) {
+          // first occurrence wins: min key = (smallest value, smallest index);
+          // max key = (largest value, smallest index) via the complemented index
+          for (int o = 16; o > 0; o >>= 1) {
+            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+          }
+          if (lane == 0 && kmin != ~0ull) {
+            atomicMin(q.ext, kmin);
+            atomicMax(q.ext + 1, kmax);
           }
         }
       }
       if (!ok) {
         *s_err = 1;
-        atomicMax(p.err, p.tag);
+        atomicMax(L.err, L.tag);
       }
     } else {
       // MMA warp: the whole warp runs the issue loop with warp-uniform values;
       // one elected lane issues each tcgen05.mma and commit
+      const uint64_t desc0 = smem_desc_noswizzle(smem_u32(zbuf), q.zrows * 16, 128);
       const uint32_t dlo = (uint32_t)desc0, dhi = (uint32_t)(desc0 >> 32);
-      const uint32_t zoff1 = p.zplane >> 4;
-      const uint32_t kstride = 2u * p.zrows;  // one 32-byte K step of Z, in 16-byte units
+      const uint32_t zoff1 = zplane >> 4;
+      const uint32_t kstride = 2u * q.zrows;  // one 32-byte K step of Z, in 16-byte units
+      const uint32_t ksteps = q.kmma / 32;
+      const uint32_t h = q.h;
       const bool leader = elect_one();
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
@@ -411,18 +447,18 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
           break;
         }
         tc_fence_after();
-        const uint32_t r0 = st * p.rps, cnt = min(nrows, r0 + p.rps) - r0;
-        const uint32_t a_stage = tmem + a_col0 + s * p.rps * a_row_cols;
+        const uint32_t r0 = st * L.rps, cnt = min(nrows, r0 + L.rps) - r0;
+        const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
         // image row r feeds output rows n in [r-h+1, r] of the tile: the band
         // [n0, n1) rounded out to 16 (rows past the map are computed, not stored)
 #pragma unroll 4
         for (uint32_t i = 0; i < kMaxRps; ++i) {
           if (i >= cnt) break;
           const uint32_t r = r0 + i;
-          const uint32_t n0 = (r + 1 > p.h ? r + 1 - p.h : 0u) & ~15u;
-          const uint32_t n1 = min(p.NT, (r & ~15u) + 16u);
+          const uint32_t n0 = (r + 1 > h ? r + 1 - h : 0u) & ~15u;
+          const uint32_t n1 = min(L.NT, (r & ~15u) + 16u);
           const uint32_t idesc = idesc0 | (((n1 - n0) >> 3) << 17);
-          const uint32_t zrow = dlo + n0 + p.h + 15u - r;  // first Z row of the band
+          const uint32_t zrow = dlo + n0 + h + 15u - r;  // first Z row of the band
           const uint32_t a = a_stage + i * a_row_cols;
           if (leader) {
 #pragma unroll
@@ -431,7 +467,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
 #pragma unroll
               for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
                 if (kk < ksteps)
-                  mma_i8_ts(tmem + c * p.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                  mma_i8_ts(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
                             ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
               }
             }
@@ -443,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
       if (ok && leader) mma_commit(dfull);
       if (!ok && lane == 0) {
         *s_err = 1;
-        atomicMax(p.err, p.tag);
+        atomicMax(L.err, L.tag);
       }
       __syncwarp();
     }
@@ -454,61 +490,15 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const UmmaParam
   __syncthreads();
   if (mma_warp) {
     mma_commit_warp(drain);
-    if (!mbar_wait(drain, 0, global_ns() + kWaitNs) && lane == 0) atomicMax(p.err, p.tag);
+    if (!mbar_wait(drain, 0, global_ns() + kWaitNs) && lane == 0) atomicMax(L.err, L.tag);
     __syncwarp();
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
   }
 }
 
-struct Plan {
-  uint32_t kmma, ks, NT, rps, imgp, rows_max, zrows, zplane, plane_bytes, nbuf;
-  uint32_t tab_off, z_off, img_off, rs_off, smem;
-};
-
-bool make_plan(uint32_t w, uint32_t h, bool masked, Plan& pl) {
-  if (w < 8 || w > (masked ? 128u : 256u) || h < 1 || h > 128) return false;
-  const uint32_t npl = masked ? 3 : 1, ncorr = masked ? 3 : 1, nz = masked ? 2 : 1;
-  pl.kmma = (w + 31) & ~31u;
-  uint32_t ks = 8;
-  while (ks * 4 < pl.kmma) ks *= 2;
-  pl.ks = ks;
-  pl.imgp = kM + 4 * ks + 16;
-  pl.zrows = h + 32;
-  pl.zplane = (pl.kmma / 16) * pl.zrows * 16;
-  const uint32_t nts[2] = {masked ? 64u : 128u, 64u};
-  for (uint32_t nt : nts) {
-    const uint32_t tm_left = kTmemCols - ncorr * nt;
-    const uint32_t rps = tm_left / (kStages * npl * ks);
-    if (rps < 1) continue;
-    const uint32_t rows = nt + h - 1;
-    const uint32_t plane = (uint32_t)align_up((size_t)rows * pl.imgp, 128);
-    for (uint32_t nbuf : {2u, 1u}) {
-      const uint32_t tab_off = kSmemHeader;
-      const uint32_t z_off = tab_off + (uint32_t)align_up(rows * 8, 128);
-      const uint32_t img_off = z_off + (uint32_t)align_up((size_t)nz * pl.zplane, 128);
-      const uint32_t rs_off = img_off + nbuf * npl * plane;
-      const uint32_t end = rs_off + (masked ? 0u : rows * kM * 4);
-      if (end <= 227u * 1024u) {
-        pl.NT = nt;
-        pl.rps = rps > (uint32_t)kMaxRps ? (uint32_t)kMaxRps : rps;
-        pl.rows_max = rows;
-        pl.plane_bytes = plane;
-        pl.nbuf = nbuf;
-        pl.tab_off = tab_off;
-        pl.z_off = z_off;
-        pl.img_off = img_off;
-        pl.rs_off = rs_off;
-        pl.smem = end < kMinSmem ? kMinSmem : end;
-        return true;
-      }
-    }
-  }
-  return false;
-}
-
 template <int KS, bool MASKED>
-cudaError_t launch_ks(const UmmaParams& p, uint32_t smem, uint32_t grid, cudaStream_t s) {
+cudaError_t launch_ks(const UmmaLaunch& L, uint32_t smem, uint32_t grid, cudaStream_t s) {
   static bool attr_set = false;  // per instantiation, process-wide
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>,
@@ -516,8 +506,14 @@ cudaError_t launch_ks(const UmmaParams& p, uint32_t smem, uint32_t grid, cudaStr
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  umma_match_kernel<KS, MASKED><<<grid, kThreads, smem, s>>>(p);
+  umma_match_kernel<KS, MASKED><<<grid, kThreads, smem, s>>>(L);
   return cudaGetLastError();
+}
+
+template <int KS, bool MASKED>
+cudaError_t set_smem_attr() {
+  return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              227 * 1024);
 }
 
 int sm_count() {
@@ -531,71 +527,191 @@ int sm_count() {
   return n;
 }
 
+uint32_t ks_of(uint32_t w) {
+  const uint32_t kmma = (w + 31) & ~31u;
+  uint32_t ks = 8;
+  while (ks * 4 < kmma) ks *= 2;
+  return ks;
+}
+
+// Kernel-wide tile and shared-memory plan for a group sharing (ks, masked):
+// sized for the group's tallest template.
+bool make_plan(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
+  const uint32_t npl = masked ? 3 : 1, ncorr = masked ? 3 : 1, nz = masked ? 2 : 1;
+  pl.ks = ks;
+  pl.masked = masked;
+  pl.imgp = kM + 4 * ks + 16;
+  const uint32_t kmma = 4 * ks;  // largest K of the group
+  const uint32_t zplane = (kmma / 16) * (hmax + 32) * 16;
+  const uint32_t nts[2] = {masked ? 64u : 128u, 64u};
+  for (uint32_t nt : nts) {
+    const uint32_t tm_left = kTmemCols - ncorr * nt;
+    const uint32_t rps = tm_left / (kStages * npl * ks);
+    if (rps < 1) continue;
+    const uint32_t rows = nt + hmax - 1;
+    const uint32_t plane = (uint32_t)align_up((size_t)rows * pl.imgp, 128);
+    for (uint32_t nbuf : {2u, 1u}) {
+      const uint32_t z_off = kSmemHeader;
+      const uint32_t img_off = z_off + (uint32_t)align_up((size_t)nz * zplane, 128);
+      const uint32_t rs_off = img_off + nbuf * npl * plane;
+      const uint32_t end = rs_off + (masked ? 0u : rows * kM * 4);
+      if (end <= 227u * 1024u) {
+        pl.NT = nt;
+        pl.rps = rps > kMaxRps ? kMaxRps : rps;
+        pl.plane_bytes = plane;
+        pl.nbuf = nbuf;
+        pl.z_off = z_off;
+        pl.img_off = img_off;
+        pl.rs_off = rs_off;
+        pl.smem = end < kMinSmem ? kMinSmem : end;
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
 }  // namespace
 
 bool umma_supported(const MatchArgs& a) {
-  Plan pl;
   if (a.precision == IPB_PRECISION_REFERENCE_F32) return false;
   if (a.mask && !a.mask_binary) return false;  // general u8 masks: CUDA-core byte planes
-  return a.w >= 16 && a.h >= 8 && (size_t)a.w * a.h <= 33025 && make_plan(a.w, a.h, a.mask != nullptr, pl);
+  if (a.w < 16 || a.h < 8 || a.h > 128 || a.w > (a.mask ? 128u : 256u) || (size_t)a.w * a.h > 33025) return false;
+  UmmaPlan pl;
+  return make_plan(ks_of(a.w), a.mask != nullptr, a.h, pl);
 }
 
-cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag) {
-  Plan pl;
-  const bool masked = a.mask != nullptr;
-  if (!make_plan(a.w, a.h, masked, pl)) return cudaErrorNotSupported;
-  UmmaParams p;
-  p.img = a.img;
-  p.W = a.W;
-  p.H = a.H;
-  p.tpl = a.tpl;
-  p.mask = a.mask;
-  p.w = a.w;
-  p.h = a.h;
-  p.kmma = pl.kmma;
-  p.NT = pl.NT;
-  p.rps = pl.rps;
-  p.imgp = pl.imgp;
-  p.rows_max = pl.rows_max;
-  p.zrows = pl.zrows;
-  p.zplane = pl.zplane;
-  p.tab_off = pl.tab_off;
-  p.z_off = pl.z_off;
-  p.img_off = pl.img_off;
-  p.rs_off = pl.rs_off;
-  p.plane_bytes = pl.plane_bytes;
-  p.nbuf = pl.nbuf;
-  p.Wo = a.W - a.w + 1;
-  p.Ho = a.H - a.h + 1;
-  p.tiles_x = (p.Wo + kM - 1) / kM;
-  p.tiles = p.tiles_x * ((p.Ho + pl.NT - 1) / pl.NT);
-  p.method = a.method;
-  p.precision = a.precision;
-  const uintptr_t ia = reinterpret_cast<uintptr_t>(a.img);
-  p.load_mode = ((ia & 15u) == 0 && (a.W & 15u) == 0) ? 2 : (((ia & 3u) == 0 && (a.W & 3u) == 0) ? 1 : 0);
-  p.out = a.out;
-  p.err = err_word;
-  p.tag = tag;
-  const uint32_t grid = p.tiles < (uint32_t)sm_count() ? p.tiles : (uint32_t)sm_count();
+uint32_t umma_group_key(const MatchArgs& a) { return ks_of(a.w) * 2 + (a.mask ? 1 : 0); }
+
+cudaError_t umma_prepare_kernels() {
   cudaError_t e;
-  timer_begin(a.timer, kKernelUmma, a.stream);
-  if (masked) {
+  if ((e = set_smem_attr<8, false>()) != cudaSuccess || (e = set_smem_attr<16, false>()) != cudaSuccess ||
+      (e = set_smem_attr<32, false>()) != cudaSuccess || (e = set_smem_attr<64, false>()) != cudaSuccess ||
+      (e = set_smem_attr<8, true>()) != cudaSuccess || (e = set_smem_attr<16, true>()) != cudaSuccess ||
+      (e = set_smem_attr<32, true>()) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) { return make_plan(ks, masked, hmax, pl); }
+
+UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
+                         unsigned long long* ext_keys) {
+  UmmaProblem q{};
+  q.img = a.img;
+  q.tpl = a.tpl;
+  q.mask = a.mask;
+  q.out = a.out;
+  q.ext = ext_keys;
+  q.W = a.W;
+  q.H = a.H;
+  q.w = a.w;
+  q.h = a.h;
+  q.Wo = a.W - a.w + 1;
+  q.Ho = a.H - a.h + 1;
+  q.tiles_x = (q.Wo + kM - 1) / kM;
+  q.tile_begin = tile_begin;
+  q.kmma = (a.w + 31) & ~31u;
+  q.zrows = a.h + 32;
+  q.rows_max = pl.NT + a.h - 1;
+  const uintptr_t ia = reinterpret_cast<uintptr_t>(a.img);
+  q.load_mode = ((ia & 15u) == 0 && (a.W & 15u) == 0) ? 2 : (((ia & 3u) == 0 && (a.W & 3u) == 0) ? 1 : 0);
+  q.method = a.method;
+  q.precision = a.precision;
+  return q;
+}
+
+uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl) {
+  return q.tiles_x * ((q.Ho + pl.NT - 1) / pl.NT);
+}
+
+cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t stream, KernelTimer* timer) {
+  L.NT = pl.NT;
+  L.rps = pl.rps;
+  L.imgp = pl.imgp;
+  L.plane_bytes = pl.plane_bytes;
+  L.nbuf = pl.nbuf;
+  L.z_off = pl.z_off;
+  L.img_off = pl.img_off;
+  L.rs_off = pl.rs_off;
+  if (L.tiles == 0) return cudaSuccess;
+  const uint32_t grid = L.tiles < (uint32_t)sm_count() ? L.tiles : (uint32_t)sm_count();
+  cudaError_t e;
+  timer_begin(timer, kKernelUmma, stream);
+  if (pl.masked) {
     switch (pl.ks) {
-      case 8: e = launch_ks<8, true>(p, pl.smem, grid, a.stream); break;
-      case 16: e = launch_ks<16, true>(p, pl.smem, grid, a.stream); break;
-      default: e = launch_ks<32, true>(p, pl.smem, grid, a.stream); break;
+      case 8: e = launch_ks<8, true>(L, pl.smem, grid, stream); break;
+      case 16: e = launch_ks<16, true>(L, pl.smem, grid, stream); break;
+      default: e = launch_ks<32, true>(L, pl.smem, grid, stream); break;
     }
   } else {
     switch (pl.ks) {
-      case 8: e = launch_ks<8, false>(p, pl.smem, grid, a.stream); break;
-      case 16: e = launch_ks<16, false>(p, pl.smem, grid, a.stream); break;
-      case 32: e = launch_ks<32, false>(p, pl.smem, grid, a.stream); break;
-      default: e = launch_ks<64, false>(p, pl.smem, grid, a.stream); break;
+      case 8: e = launch_ks<8, false>(L, pl.smem, grid, stream); break;
+      case 16: e = launch_ks<16, false>(L, pl.smem, grid, stream); break;
+      case 32: e = launch_ks<32, false>(L, pl.smem, grid, stream); break;
+      default: e = launch_ks<64, false>(L, pl.smem, grid, stream); break;
     }
   }
   count_launch(kKernelUmma);
-  timer_end(a.timer, a.stream);
+  timer_end(timer, stream);
   return e;
+}
+
+cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag) {
+  UmmaPlan pl;
+  if (!make_plan(ks_of(a.w), a.mask != nullptr, a.h, pl)) return cudaErrorNotSupported;
+  UmmaLaunch L{};
+  L.inl[0] = umma_problem(a, pl, 0, nullptr);
+  L.nprobs = 1;
+  L.tiles = umma_problem_tiles(L.inl[0], pl);
+  L.err = err_word;
+  L.tag = tag;
+  return launch_umma_batch(pl, L, a.stream, a.timer);
+}
+
+// ---- fused find_extremes bookkeeping ---------------------------------------
+__global__ void extremes_keys_init_kernel(unsigned long long* keys, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    keys[2 * i] = ~0ull;
+    keys[2 * i + 1] = 0ull;
+  }
+}
+
+// keys -> ipb_extremes_f32 (the order key inverts exactly; indices -> (x, y))
+__global__ void extremes_keys_finish_kernel(const unsigned long long* keys, const uint32_t* widths,
+                                            ipb_extremes_f32* const* outs, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !outs[i]) return;
+  const unsigned long long kmin = keys[2 * i], kmax = keys[2 * i + 1];
+  auto value = [](uint32_t ok) {
+    const uint32_t b = (ok & 0x80000000u) ? (ok & 0x7FFFFFFFu) : ~ok;
+    return __uint_as_float(b);
+  };
+  const uint32_t imin = (uint32_t)kmin, imax = 0xFFFFFFFFu - (uint32_t)kmax;
+  ipb_extremes_f32 r;
+  r.max_value = value((uint32_t)(kmax >> 32));
+  r.min_value = value((uint32_t)(kmin >> 32));
+  r.max_value_location_x = imax % widths[i];
+  r.max_value_location_y = imax / widths[i];
+  r.min_value_location_x = imin % widths[i];
+  r.min_value_location_y = imin / widths[i];
+  *outs[i] = r;
+}
+
+cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  extremes_keys_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, n);
+  count_launch(kKernelExtremes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const uint32_t* widths,
+                                        ipb_extremes_f32* const* outs, uint32_t n, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  extremes_keys_finish_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, widths, outs, n);
+  count_launch(kKernelExtremes);
+  return cudaGetLastError();
 }
 
 }  // namespace ipb

@@ -71,3 +71,120 @@ def find_extremes_device(image: torch.Tensor, stream=None) -> Extremes:
     return Extremes(res.max_value, res.min_value,
                     (res.max_value_location_x, res.max_value_location_y),
                     (res.min_value_location_x, res.min_value_location_y))
+
+
+# ---- batches ------------------------------------------------------------------
+
+class _Pair(C.Structure):
+    _fields_ = [
+        ("image", C.c_void_p), ("image_width", C.c_uint32), ("image_height", C.c_uint32),
+        ("templ", C.c_void_p), ("template_width", C.c_uint32), ("template_height", C.c_uint32),
+        ("mask", C.c_void_p), ("mask_width", C.c_uint32), ("mask_height", C.c_uint32),
+        ("mask_is_binary", C.c_int), ("method", C.c_int),
+        ("out", C.c_void_p), ("extremes", C.c_void_p),
+    ]
+
+
+EXTREMES_DTYPE = [("max_value", "<f4"), ("min_value", "<f4"), ("max_x", "<u4"), ("max_y", "<u4"),
+                  ("min_x", "<u4"), ("min_y", "<u4")]
+
+
+def _bind_batch():
+    L = _lib.lib()
+    if getattr(L, "_batch_bound", False):
+        return L
+    L.ipb_match_template_batch_device.argtypes = [C.POINTER(_Pair), C.c_uint32, C.c_int, C.c_void_p]
+    L.ipb_match_template_batch_device.restype = C.c_int
+    L.ipb_batch_plan_create.argtypes = [C.POINTER(_Pair), C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]
+    L.ipb_batch_plan_create.restype = C.c_int
+    L.ipb_batch_plan_launch.argtypes = [C.c_void_p, C.c_void_p]
+    L.ipb_batch_plan_launch.restype = C.c_int
+    L.ipb_batch_plan_info.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.ipb_batch_plan_info.restype = C.c_int
+    L.ipb_batch_plan_destroy.argtypes = [C.c_void_p]
+    L.ipb_batch_plan_destroy.restype = C.c_int
+    L._batch_bound = True
+    return L
+
+
+class Batch:
+    """A batch of (image, template[, mask], method) pairs on the device.
+
+    ``items``: sequence of ``(image, template, method)`` or
+    ``(image, template, method, mask)`` CUDA uint8 tensors. Score maps are
+    allocated here (``self.outs``) and, with ``extremes=True``, each map's
+    find_extremes record is written on the device into ``self.extremes``
+    (an int32 tensor of n x 6 words; see :meth:`extremes_host`).
+    """
+
+    def __init__(self, items, *, extremes: bool = True, masks_binary: bool = True):
+        self.items = list(items)
+        dev = self.items[0][0].device if self.items else torch.device("cuda")
+        self.outs = []
+        n = len(self.items)
+        self.extremes = torch.zeros((max(n, 1), 6), dtype=torch.int32, device=dev)
+        self._pairs = (_Pair * max(n, 1))()
+        for i, it in enumerate(self.items):
+            image, template, method = it[0], it[1], it[2]
+            mask = it[3] if len(it) > 3 else None
+            _check_gray(image, "image")
+            _check_gray(template, "template")
+            H, W = image.shape
+            h, w = template.shape
+            out = torch.empty((max(H - h + 1, 1), max(W - w + 1, 1)), dtype=torch.float32,
+                              device=image.device)
+            self.outs.append(out)
+            p = self._pairs[i]
+            p.image, p.image_width, p.image_height = image.data_ptr(), W, H
+            p.templ, p.template_width, p.template_height = template.data_ptr(), w, h
+            if mask is not None:
+                _check_gray(mask, "mask")
+                p.mask, p.mask_height, p.mask_width = mask.data_ptr(), mask.shape[0], mask.shape[1]
+                p.mask_is_binary = int(masks_binary)
+            p.method = int(MatchTemplateMethod(method))
+            p.out = out.data_ptr()
+            p.extremes = (self.extremes.data_ptr() + 24 * i) if extremes else None
+
+    def run(self, precision: Precision | int = Precision.ExactFp64, stream=None):
+        """One-shot batch (returns when the batch has completed)."""
+        L = _bind_batch()
+        check(L.ipb_match_template_batch_device(self._pairs, len(self.items), int(precision),
+                                                _stream_handle(stream)))
+        return self.outs
+
+    def extremes_host(self):
+        """The find_extremes records as a list of Extremes."""
+        import numpy as np
+        raw = self.extremes[: len(self.items)].cpu().numpy().view(np.dtype(EXTREMES_DTYPE)).reshape(-1)
+        return [Extremes(float(r["max_value"]), float(r["min_value"]), (int(r["max_x"]), int(r["max_y"])),
+                         (int(r["min_x"]), int(r["min_y"]))) for r in raw]
+
+
+class BatchPlan:
+    """A planned batch replayed as a CUDA graph (ipb_batch_plan_*)."""
+
+    def __init__(self, batch: Batch, precision: Precision | int = Precision.ExactFp64):
+        L = _bind_batch()
+        self.batch = batch
+        self._h = C.c_void_p()
+        check(L.ipb_batch_plan_create(batch._pairs, len(batch.items), int(precision), C.byref(self._h)))
+
+    def launch(self, stream=None):
+        check(_bind_batch().ipb_batch_plan_launch(self._h, _stream_handle(stream)))
+        return self.batch.outs
+
+    def info(self):
+        k, t = C.c_uint32(), C.c_uint32()
+        check(_bind_batch().ipb_batch_plan_info(self._h, C.byref(k), C.byref(t)))
+        return {"kernels": k.value, "tensor_pairs": t.value}
+
+    def close(self):
+        if self._h:
+            _bind_batch().ipb_batch_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

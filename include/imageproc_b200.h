@@ -192,6 +192,50 @@ ipb_status ipb_match_template_device_noalloc(
     int mask_is_binary, int method, int precision, float *d_out,
     void *stream);
 
+/* ---- batches --------------------------------------------------------------
+ * Many (image, template[, mask]) pairs of uneven sizes and methods in one
+ * call: the reference's match_template / match_template_with_mask
+ * (src/template_matching.rs:78, :125) applied per pair, optionally followed
+ * by find_extremes (:479) of each score map. Additive API (the reference has
+ * no batch form). Pairs are checked in order with the reference's assertions
+ * before any work; the first failing pair's status is returned and its index
+ * named in the message. Tensor-core pairs of equal tensor-memory row width
+ * share one persistent launch each; find_extremes is fused into their
+ * epilogue. */
+
+typedef struct ipb_extremes_f32 ipb_extremes_f32;
+
+typedef struct ipb_pair {
+    const uint8_t *image; /* device */
+    uint32_t image_width, image_height;
+    const uint8_t *templ; /* device */
+    uint32_t template_width, template_height;
+    const uint8_t *mask; /* device, NULL = unmasked */
+    uint32_t mask_width, mask_height;
+    int mask_is_binary; /* every mask value is 0 or 1 */
+    int method;
+    float *out;                  /* device score map */
+    ipb_extremes_f32 *extremes;  /* device record filled with find_extremes(out), or NULL */
+} ipb_pair;
+
+/* Enqueue the whole batch on `stream`. */
+ipb_status ipb_match_template_batch_device(const ipb_pair *pairs, uint32_t n,
+                                           int precision, void *stream);
+
+/* A reusable batch: pairs checked, kernel paths chosen (by the autotuner when
+ * the environment variable IPB_AUTOTUNE=1, else by its cost model), device
+ * descriptors uploaded and the launch sequence captured in a CUDA graph.
+ * Pointers in `pairs` must stay valid for the plan's life; launching replays
+ * the graph on `stream`. */
+typedef struct ipb_batch_plan ipb_batch_plan;
+ipb_status ipb_batch_plan_create(const ipb_pair *pairs, uint32_t n, int precision,
+                                 ipb_batch_plan **plan);
+ipb_status ipb_batch_plan_launch(ipb_batch_plan *plan, void *stream);
+/* Kernels one launch of the plan runs, and how many pairs use tensor cores. */
+ipb_status ipb_batch_plan_info(const ipb_batch_plan *plan, uint32_t *kernels,
+                               uint32_t *tensor_pairs);
+ipb_status ipb_batch_plan_destroy(ipb_batch_plan *plan);
+
 /* ---- find_extremes -------------------------------------------------------- */
 
 /* Extremes<T> (src/template_matching.rs:463-475), field order kept. */

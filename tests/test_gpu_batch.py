@@ -1,0 +1,139 @@
+"""Batched matching (one persistent launch per tensor-core group, CUDA graphs)
+against the oracle, including the fused find_extremes.
+
+Bar: every score map bit-exact against the oracle's exact-sum epilogue, every
+extremes record equal to the oracle's find_extremes of that map (first
+occurrence on ties, src/template_matching.rs:494-503).
+"""
+
+import numpy as np
+import pytest
+
+from imageproc_b200 import _lib, synthetic
+from imageproc_b200 import template_matching as tm
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def _mixed_items(seed, n):
+    """Uneven pairs: tensor-core shapes of every row width, CUDA-core shapes
+    (templates narrower than 16 or general masks), binary masks, all methods."""
+    g = np.random.default_rng(seed)
+    items = []
+    for k in range(n):
+        H, W = int(g.integers(40, 400)), int(g.integers(40, 700))
+        h = int(g.integers(1, min(H, 120) + 1))
+        w = int(g.integers(4, min(W, 200) + 1))
+        image = g.integers(0, 256, (H, W), dtype=np.uint8)
+        if k % 7 == 3:
+            image[:] = 200  # flat: every score ties, extremes at the first pixel
+        template = g.integers(0, 256, (h, w), dtype=np.uint8)
+        method = int(g.integers(0, 4))
+        kind = k % 3
+        mask = None
+        if kind == 1:
+            mask = (g.random((h, w)) < 0.8).astype(np.uint8)
+        items.append((image, template, method, mask))
+    return items
+
+
+def _to_device(items):
+    import torch
+    dev = []
+    for image, template, method, mask in items:
+        t = (torch.from_numpy(image).cuda(), torch.from_numpy(template).cuda(), method)
+        if mask is not None:
+            t = t + (torch.from_numpy(mask).cuda(),)
+        dev.append(t)
+    return dev
+
+
+def _check(items, outs, extremes):
+    for k, ((image, template, method, mask), out, ex) in enumerate(zip(items, outs, extremes)):
+        got = out.cpu().numpy()
+        exp = O.match_exact(image, template, method, mask, precision=0)
+        bad = np.argwhere(bits(got) != bits(exp))
+        assert bad.size == 0, (k, image.shape, template.shape, method, mask is not None, bad[:3])
+        mx, mn, mxl, mnl = O.find_extremes(exp)
+        assert (ex.max_value, ex.min_value, ex.max_value_location, ex.min_value_location) == \
+            (float(mx), float(mn), mxl, mnl), k
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_batch_mixed_pairs_bit_exact_with_fused_extremes(seed):
+    from imageproc_b200 import device
+    items = _mixed_items(seed, 20)
+    batch = device.Batch(_to_device(items))
+    batch.run()
+    _check(items, batch.outs, batch.extremes_host())
+
+
+def test_batch_plan_graph_replay():
+    import torch
+
+    from imageproc_b200 import device
+    items = _mixed_items(7, 12)
+    batch = device.Batch(_to_device(items))
+    plan = device.BatchPlan(batch)
+    info = plan.info()
+    assert info["tensor_pairs"] >= 1 and info["kernels"] >= 1
+    n0 = _lib.launch_count()
+    for _ in range(2):
+        for o in batch.outs:
+            o.fill_(float("nan"))
+        batch.extremes.zero_()
+        plan.launch()
+        torch.cuda.synchronize()
+        _check(items, batch.outs, batch.extremes_host())
+    assert _lib.launch_count() - n0 == 2 * info["kernels"]
+    plan.close()
+
+
+def test_batch_of_more_problems_than_fit_in_kernel_parameters():
+    # > 8 tensor pairs of one group: problem descriptors come from device memory
+    from imageproc_b200 import device
+    g = np.random.default_rng(3)
+    items = []
+    for k in range(13):
+        H, W = int(g.integers(64, 300)), int(g.integers(64, 500))
+        image = g.integers(0, 256, (H, W), dtype=np.uint8)
+        template = g.integers(0, 256, (int(g.integers(8, 60)), int(g.integers(33, 64))), dtype=np.uint8)
+        items.append((image, template, k % 4, None))
+    batch = device.Batch(_to_device(items))
+    plan = device.BatchPlan(batch)
+    assert plan.info()["tensor_pairs"] == 13
+    plan.launch()
+    import torch
+    torch.cuda.synchronize()
+    _check(items, batch.outs, batch.extremes_host())
+    plan.close()
+
+
+def test_uneven_pairs_workload_reduced():
+    # the batched workload's generator at reduced image sides, all pairs checked
+    from imageproc_b200 import device
+    pairs = synthetic.uneven_pairs(n=24, seed=3, lo=128, hi=768)
+    items = [(im, tp, m, None) for im, tp, m in pairs]
+    batch = device.Batch(_to_device(items))
+    batch.run()
+    _check(items, batch.outs, batch.extremes_host())
+
+
+def test_batch_rejects_invalid_pair_before_any_work():
+    import torch
+
+    from imageproc_b200 import device
+    img = torch.zeros((10, 10), dtype=torch.uint8, device="cuda")
+    ok_t = torch.zeros((3, 3), dtype=torch.uint8, device="cuda")
+    bad_t = torch.zeros((3, 12), dtype=torch.uint8, device="cuda")
+    batch = device.Batch([(img, ok_t, 0), (img, bad_t, 0)])
+    batch.outs[0].fill_(-1.0)
+    with pytest.raises(tm.Panic, match="^pair 1: image width must be greater than or equal to template width$"):
+        batch.run()
+    torch.cuda.synchronize()
+    assert (batch.outs[0] == -1.0).all()
