@@ -90,7 +90,7 @@ void note_timed(KernelTimer* t, double macs, double bytes) {
 const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
-      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8"};
+      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -154,6 +154,7 @@ struct Context {
   DevBuf scratch, ext_scratch, ext_result, img, tpl, mask, out;
   void* pinned = nullptr;  // small pinned host block: reduction results, error words
   DevBuf errw;                     // tensor-core error word (largest failing launch tag)
+  DevBuf many_keys;                // per-template extremes keys of the many-templates path
   unsigned int tag = 0;            // tag of the last tensor-core launch
   unsigned int tag_checked = 0;    // largest failing tag already reported
   bool tensor_since_check = false;
@@ -161,7 +162,7 @@ struct Context {
     if (device < 0) return;
     cudaSetDevice(device);
     if (last) cudaEventSynchronize(last);
-    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw})
+    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys})
       if (b->p) cudaFree(b->p);
     if (pinned) cudaFreeHost(pinned);
     if (last) cudaEventDestroy(last);
@@ -462,6 +463,41 @@ IPB_API ipb_status ipb_match_template_with_mask_parallel(const uint8_t* image, u
                                                          uint32_t mh, float* out) {
   if (!mask) return fail(IPB_ERR_INVALID_ARGUMENT, "null mask");
   return host_match(image, W, H, tpl, w, h, method, mask, mw, mh, out);
+}
+
+IPB_API ipb_status ipb_match_templates_device(const uint8_t* d_image, uint32_t W, uint32_t H,
+                                              const uint8_t* d_templates, uint32_t w, uint32_t h, uint32_t n,
+                                              int method, int precision, float* d_out,
+                                              ipb_extremes_f32* d_extremes, void* stream) {
+  ipb_status st = check_match(W, H, w, h, false, 0, 0, method);
+  if (st) return st;
+  if (precision < 0 || precision > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!many_supported(w, h, n, precision))
+    return fail(IPB_ERR_INVALID_ARGUMENT,
+                "ipb_match_templates_device takes 16..64 x 1..64 templates in an exact precision; use "
+                "ipb_match_template_batch_device for other shapes");
+  if (!d_image || !d_templates || (!d_out && !d_extremes)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  if ((st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
+  if (d_extremes && (st = ensure(c, c->many_keys, sizeof(unsigned long long) * 2 * n))) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  IPB_CUDA(cudaStreamWaitEvent(s, c->last, 0), "cudaStreamWaitEvent");
+  unsigned long long* keys = d_extremes ? static_cast<unsigned long long*>(c->many_keys.p) : nullptr;
+  if (keys) IPB_CUDA(launch_many_keys_init(keys, n, s), "extremes init");
+  c->tag += 1;
+  c->tensor_since_check = true;
+  KernelTimer* t = acquire_timer();
+  const cudaError_t e = launch_many(d_image, W, H, d_templates, w, h, n, method, precision, d_out, keys,
+                                    static_cast<unsigned int*>(c->errw.p), c->tag, s, t);
+  if (t) {
+    const double Wo = W - w + 1.0, Ho = H - h + 1.0, tp = (double)w * h;
+    note_timed(t, Wo * Ho * tp * n, (double)W * H + tp * n + (d_out ? 4.0 * Wo * Ho * n : 0.0));
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "many-templates launch");
+  if (keys) IPB_CUDA(launch_many_keys_finish(keys, W - w + 1, d_extremes, n, s), "extremes finish");
+  IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
+  return IPB_OK;
 }
 
 IPB_API ipb_status ipb_match_template_device(const uint8_t* d_image, uint32_t W, uint32_t H,

@@ -20,6 +20,7 @@ enum KernelId : int {
   kKernelReference,
   kKernelExtremes,
   kKernelUmma,
+  kKernelMany,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -141,6 +142,15 @@ cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t st
 cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s);
 cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const uint32_t* widths,
                                         ipb_extremes_f32* const* outs, uint32_t n, cudaStream_t s);
+
+// ---- many templates of one size against one image (tm_many.cu) ------------
+bool many_supported(uint32_t w, uint32_t h, uint32_t n, int precision);
+cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_t* tpl, uint32_t w, uint32_t h,
+                        uint32_t n, int method, int precision, float* out, unsigned long long* ext_keys,
+                        unsigned int* err, unsigned int tag, cudaStream_t stream, KernelTimer* timer);
+cudaError_t launch_many_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s);
+cudaError_t launch_many_keys_finish(const unsigned long long* keys, uint32_t Wo, ipb_extremes_f32* out, uint32_t n,
+                                    cudaStream_t s);
 
 // ---- reference-order f32 kernel (tm_reference.cu) -------------------------
 size_t reference_scratch_bytes(const MatchArgs& a);

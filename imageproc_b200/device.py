@@ -188,3 +188,42 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+def match_templates_device(image: torch.Tensor, templates: torch.Tensor, method, *,
+                           precision: Precision | int = Precision.ExactFp64, scores: bool = True,
+                           extremes: bool = False, out: torch.Tensor | None = None, stream=None):
+    """Score n templates of one size (an (n, h, w) uint8 CUDA tensor) against
+    one image in one tensor-core launch (ipb_match_templates_device).
+
+    Returns ``(scores, extremes)``: scores is position-major, shape
+    (H - h + 1, W - w + 1, n) (None when ``scores=False``); extremes is a list
+    of n :class:`Extremes` (None unless ``extremes=True``)."""
+    L = _lib.lib()
+    if not getattr(L, "_many_bound", False):
+        L.ipb_match_templates_device.argtypes = [
+            C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+            C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ipb_match_templates_device.restype = C.c_int
+        L._many_bound = True
+    _check_gray(image, "image")
+    if templates.dtype != torch.uint8 or templates.dim() != 3 or not templates.is_cuda or \
+            not templates.is_contiguous():
+        raise TypeError("templates must be a contiguous (n, h, w) uint8 CUDA tensor")
+    H, W = image.shape
+    n, h, w = templates.shape
+    if scores and out is None:
+        out = torch.empty((max(H - h + 1, 1), max(W - w + 1, 1), n), dtype=torch.float32,
+                          device=image.device)
+    ext = torch.zeros((n, 6), dtype=torch.int32, device=image.device) if extremes else None
+    check(L.ipb_match_templates_device(
+        image.data_ptr(), W, H, templates.data_ptr(), w, h, n, int(MatchTemplateMethod(method)),
+        int(precision), out.data_ptr() if scores else None, ext.data_ptr() if extremes else None,
+        _stream_handle(stream)))
+    ex = None
+    if extremes:
+        import numpy as np
+        raw = ext.cpu().numpy().view(np.dtype(EXTREMES_DTYPE)).reshape(-1)
+        ex = [Extremes(float(r["max_value"]), float(r["min_value"]), (int(r["max_x"]), int(r["max_y"])),
+                       (int(r["min_x"]), int(r["min_y"]))) for r in raw]
+    return (out if scores else None), ex

@@ -236,6 +236,23 @@ ipb_status ipb_batch_plan_info(const ipb_batch_plan *plan, uint32_t *kernels,
                                uint32_t *tensor_pairs);
 ipb_status ipb_batch_plan_destroy(ipb_batch_plan *plan);
 
+/* ---- many templates against one image --------------------------------------
+ * match_template (src/template_matching.rs:78-92) of n templates of one size
+ * w x h against one image, unmasked, in one launch on the tensor cores
+ * (additive API). d_templates holds the n w x h GrayImages back to back.
+ * Scores are POSITION-MAJOR: the score of template t at (x, y) is
+ * d_out[((size_t)y * (W - w + 1) + x) * n + t]. d_out may be NULL when only
+ * d_extremes (n records, find_extremes of each template's map,
+ * src/template_matching.rs:479-511) is wanted. Templates of 16..64 columns
+ * and 1..64 rows, EXACT precisions; other shapes go through
+ * ipb_match_template_batch_device. Enqueued on `stream`. */
+ipb_status ipb_match_templates_device(const uint8_t *d_image, uint32_t image_width,
+                                      uint32_t image_height, const uint8_t *d_templates,
+                                      uint32_t template_width, uint32_t template_height,
+                                      uint32_t n_templates, int method, int precision,
+                                      float *d_out, ipb_extremes_f32 *d_extremes,
+                                      void *stream);
+
 /* ---- find_extremes -------------------------------------------------------- */
 
 /* Extremes<T> (src/template_matching.rs:463-475), field order kept. */
