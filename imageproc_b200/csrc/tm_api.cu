@@ -477,6 +477,8 @@ IPB_API ipb_status ipb_match_templates_device(const uint8_t* d_image, uint32_t W
                 "ipb_match_templates_device takes 16..64 x 1..64 templates in an exact precision; use "
                 "ipb_match_template_batch_device for other shapes");
   if (!d_image || !d_templates || (!d_out && !d_extremes)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (d_extremes && (uint64_t)(W - w + 1) * (H - h + 1) > 0xFFFFFFFFull)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "fused extremes take score maps of fewer than 2^32 positions");
   Context* c = nullptr;
   if ((st = get_ctx(&c))) return st;
   if ((st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;

@@ -4,24 +4,33 @@
 // src/template_matching.rs:78-92). For a bank of templates the work becomes
 // one GEMM per output column x:
 //   D[m][t] = sum_{dy,dx} I[y0 + m + dy][x + dx] * T_t[dy][dx]
-// with M = 128 consecutive output rows, N = a block of NB templates and
+// over 128 consecutive output rows m, a block of templates t and
 // K = the template's pixels in (dy, dx) order, 32 bytes per MMA step.
 //
-// A operand: a "strip" of the image for column x -- for each 16-byte column
-// chunk j, the rows y0 .. y0 + 127 + h - 1 of bytes [x + 16j, x + 16j + 16),
-// stored 16 bytes per row in the canonical no-swizzle K-major layout. The A
-// tile for template row dy is the same strip started dy rows (16*dy bytes)
-// later, so one strip (about 5 KB) serves all h template rows.
-// B operand: the template block, K-major, resident in shared memory for the
-// CTA's lifetime. Every MMA is M128 x N128 x K32 (full tensor-core rate).
+// Image operand: a "strip" of the image for column x -- for each 16-byte
+// column chunk j, the rows y0 .. y0 + 127 + h - 1 of bytes [x + 16j,
+// x + 16j + 16), stored 16 bytes per row in the canonical no-swizzle K-major
+// layout. The operand for template row dy is the same strip started dy rows
+// (16*dy bytes) later, so one strip (about 5 KB) serves all h template rows.
+// Template operand: the template block, K-major, resident in shared memory
+// for the CTA's lifetime.
+//
+// Two operand assignments:
+//  * templates as M (kTplM): A = 128 templates, B = the strip (N = 128
+//    positions). Tensor-memory lanes are templates, so each epilogue store
+//    instruction writes 32 consecutive templates of one position -- a full
+//    128-byte line of the position-major output -- and every lane keeps its
+//    template's extremes in registers. Used when a block of 128 templates
+//    fits in shared memory (h * round32(w) <= about 1200 bytes).
+//  * positions as M: A = the strip (M = 128 positions), B = NB templates
+//    (a multiple of 16, at most 112), for larger templates.
 //
 // Roles: 4 builder warps stage the image tile (cp.async), compute the window
 // sums Y = sum I^2 of every position of the tile, and build strips; one warp
-// issues the MMAs (elected lane); 8 epilogue warps read the accumulator
-// (double-buffered in tensor memory), apply the method, write the scores and
-// fold them into per-template extremes. Scores are position-major:
-// out[(y * Wo + x) * n_templates + t], so each thread writes its 16
-// consecutive template scores as one contiguous 64-byte run.
+// issues the MMAs (warp-uniform loop, one elected lane); 8 epilogue warps
+// read the accumulator (double-buffered in tensor memory), apply the method,
+// write the scores and fold them into per-template extremes. Scores are
+// position-major: out[(y * Wo + x) * n_templates + t].
 // Every wait is bounded (2 s) and reports through the error word.
 #include "tm_common.cuh"
 #include "tm_internal.h"
@@ -32,7 +41,7 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kM = 128;           // output rows per tile (tensor-memory lanes)
+constexpr int kM = 128;           // output rows per tile
 constexpr int kXT = 32;           // output columns per tile
 constexpr int kBuildWarps = 4;
 constexpr int kEpiWarps = 8;
@@ -48,13 +57,13 @@ struct ManyParams {
   const uint8_t* tpl;  // n templates of w x h, contiguous
   uint32_t w, h, n;
   uint32_t kw;       // w rounded up to 32
-  uint32_t NB;       // templates per block (N of the MMA), multiple of 16, <= 128
+  uint32_t NB;       // templates per block: 128 (templates as M) or a multiple of 16
   uint32_t nblocks;  // ceil(n / NB)
   uint32_t Wo, Ho, bands, xtiles, spatial;  // spatial tiles = bands * xtiles
   uint32_t rows;     // strip rows: 128 + h - 1
   uint32_t ip;       // staged image row pitch
-  uint32_t b_off, tss_off, img_off, strip_off, y_off, v_off, ext_off;
-  int method, precision, vec4;  // vec4: 16-byte score stores
+  uint32_t b_off, tss_off, img_off, strip_off, y_off, v_off, ext_off, ry_off;
+  int method, precision, vec4;  // vec4: 16-byte score stores (positions as M)
   int img16;                    // image rows 16-byte aligned: cp.async staging
   float* out;                 // may be null (extremes only)
   unsigned long long* ext;    // 2 keys per template or null
@@ -73,6 +82,194 @@ __device__ __forceinline__ uint32_t order_key(float f) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// State of an epilogue warp for one tile.
+struct EpiCtx {
+  const ManyParams* p;
+  uint32_t tmem;
+  uint64_t* dfull;
+  uint64_t* dempty;
+  const uint32_t* s_y;
+  const uint32_t* s_tss;
+  unsigned long long* s_ext;
+  double* s_ry;  // [kEpiWarps][kM / 2] reciprocal roots of the strip's Y (templates as M)
+  uint32_t gx, nx, x0, y0, t0, nt;
+  uint32_t e;  // epilogue warp index 0..7: lane quadrant e & 3, half e >> 2
+  uint32_t lane;
+  unsigned long long deadline;
+  unsigned long long kmin, kmax;  // templates as M: this lane's running extremes keys
+};
+
+// Drains the tile's accumulators with the method and precision fixed at
+// compile time, so the 16 scores of a tensor-memory load are independent
+// straight-line code. Returns false when a wait ran out.
+template <bool kTplM, int kMethod, int kPrec, bool kExt>
+__device__ __forceinline__ bool epilogue(EpiCtx& c) {
+  const ManyParams& p = *c.p;
+  const uint32_t q = c.e & 3;
+  if constexpr (kTplM) {
+    // lanes are templates; this warp takes half of the tile's 128 positions
+    const uint32_t mb = (c.e >> 2) * (kM / 2);
+    const uint32_t tl = q * 32 + c.lane;
+    const bool t_ok = tl < c.nt;
+    const uint32_t tss = c.s_tss[tl];
+    // EXACT_FP64 normalisation: 1/sqrt(Y) once per position (shared by the
+    // warp's 32 templates) and 1/sqrt(T) once per lane
+    constexpr bool kNormW = method_is_norm(kMethod) && kPrec == IPB_PRECISION_EXACT_FP64;
+    double* s_ryw = c.s_ry + c.e * (kM / 2);
+    const double rT = (kNormW && tss) ? rsqrt_u32(tss) : 0.0;
+    const int mvalid = (int)p.Ho - (int)(c.y0 + mb);  // positions of the half inside the map
+    const size_t rstride = (size_t)p.Wo * p.n;
+    for (uint32_t xi = 0; xi < c.nx; ++xi) {
+      const uint32_t g = c.gx + xi, d = g & 1u;
+      if (!mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline)) return false;
+      tc_fence_after();
+      const uint32_t x = c.x0 + xi;
+      const uint32_t* ycol = c.s_y + xi * kM + mb;
+      float* ocol = (p.out && t_ok) ? p.out + ((size_t)(c.y0 + mb) * p.Wo + x) * p.n + c.t0 + tl : nullptr;
+      const uint32_t idx0 = (c.y0 + mb) * p.Wo + x;
+      if constexpr (kNormW) {
+        __syncwarp();
+        for (uint32_t i = c.lane; i < (uint32_t)kM / 2; i += 32) {
+          const uint32_t yv = ycol[i];
+          s_ryw[i] = yv ? rsqrt_u32(yv) : 0.0;
+        }
+        __syncwarp();
+      }
+      for (int cc = 0; cc < kM / 2; cc += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + mb + cc), v);
+        uint32_t Y[16];
+#pragma unroll
+        for (int k = 0; k < 16; k += 4) {
+          const uint4 y4 = *reinterpret_cast<const uint4*>(ycol + cc + k);
+          Y[k] = y4.x;
+          Y[k + 1] = y4.y;
+          Y[k + 2] = y4.z;
+          Y[k + 3] = y4.w;
+        }
+        tmem_wait_ld();
+        auto one = [&](int k) {
+          float f;
+          if constexpr (kNormW) {
+            const uint32_t score = method_is_sse(kMethod) ? (Y[k] + tss - 2u * v[k]) : v[k];
+            f = norm_quotient_fp64_w(score, __dmul_rn(s_ryw[cc + k], rT), Y[k], tss);
+          } else {
+            f = finish_score32(kMethod, kPrec, v[k], Y[k], tss);
+          }
+          if (ocol) ocol[(size_t)(cc + k) * rstride] = f;
+          if constexpr (kExt) {
+            if (t_ok) {
+              const unsigned long long key = (unsigned long long)order_key(f) << 32;
+              const uint32_t idx = idx0 + (uint32_t)(cc + k) * p.Wo;
+              c.kmin = min(c.kmin, key | idx);
+              c.kmax = max(c.kmax, key | (0xFFFFFFFFu - idx));
+            }
+          }
+        };
+        if (cc + 16 <= mvalid) {
+#pragma unroll
+          for (int k = 0; k < 16; ++k) one(k);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; ++k)
+            if (cc + k < mvalid) one(k);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&c.dempty[d]);
+    }
+    return true;
+  } else {
+    // lanes are positions (rows); this warp takes half of the block's templates
+    const uint32_t m = q * 32 + c.lane, y = c.y0 + m;
+    const uint32_t ncol = p.NB / 2, c0 = (c.e >> 2) * ncol;
+    const bool row_ok = y < p.Ho;
+    for (uint32_t xi = 0; xi < c.nx; ++xi) {
+      const uint32_t g = c.gx + xi, d = g & 1u;
+      if (!mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline)) return false;
+      tc_fence_after();
+      const uint32_t x = c.x0 + xi;
+      const uint32_t Y = c.s_y[xi * kM + m];
+      float* orow = p.out ? p.out + ((size_t)y * p.Wo + x) * p.n + c.t0 : nullptr;
+      for (uint32_t cc = c0; cc < c0 + ncol; cc += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + cc), v);
+        tmem_wait_ld();
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) f[k] = finish_score32(kMethod, kPrec, v[k], Y, c.s_tss[cc + k]);
+        if (orow && row_ok) {
+          if (p.vec4 && cc + 16 <= c.nt) {
+#pragma unroll
+            for (int k = 0; k < 16; k += 4)
+              *reinterpret_cast<float4*>(orow + cc + k) = make_float4(f[k], f[k + 1], f[k + 2], f[k + 3]);
+          } else {
+            for (int k = 0; k < 16; ++k)
+              if (cc + k < c.nt) orow[cc + k] = f[k];
+          }
+        }
+        if constexpr (kExt) {
+          // per template: smallest / largest value over this warp's 32 rows,
+          // the lowest row (= lowest linear index at this x) among ties;
+          // lane k keeps template cc + k's result
+          uint32_t my_mn = 0xFFFFFFFFu, my_ln = 0, my_mx = 0, my_lx = 0;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const uint32_t key = row_ok ? order_key(f[k]) : 0xFFFFFFFFu;
+            const uint32_t kmn = __reduce_min_sync(0xffffffffu, key);
+            const uint32_t ln = __ffs(__ballot_sync(0xffffffffu, key == kmn)) - 1;
+            const uint32_t keyx = row_ok ? order_key(f[k]) : 0u;
+            const uint32_t kmx = __reduce_max_sync(0xffffffffu, keyx);
+            const uint32_t lx = __ffs(__ballot_sync(0xffffffffu, keyx == kmx)) - 1;
+            if (c.lane == (uint32_t)k) {
+              my_mn = kmn;
+              my_ln = ln;
+              my_mx = kmx;
+              my_lx = lx;
+            }
+          }
+          if (c.lane < 16 && cc + c.lane < c.nt) {
+            const uint32_t ymn = c.y0 + q * 32 + my_ln, ymx = c.y0 + q * 32 + my_lx;
+            if (ymn < p.Ho)
+              atomicMin(&c.s_ext[2 * (cc + c.lane)], ((unsigned long long)my_mn << 32) | (ymn * p.Wo + x));
+            if (ymx < p.Ho)
+              atomicMax(&c.s_ext[2 * (cc + c.lane) + 1],
+                        ((unsigned long long)my_mx << 32) | (0xFFFFFFFFu - (ymx * p.Wo + x)));
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&c.dempty[d]);
+    }
+    return true;
+  }
+}
+
+template <bool kTplM, int kMethod>
+__device__ __forceinline__ bool epilogue_m(EpiCtx& c, bool fp64, bool ext) {
+  if constexpr (!method_is_norm(kMethod)) fp64 = true;  // precision only affects the normalisation
+  if (fp64)
+    return ext ? epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, true>(c)
+               : epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, false>(c);
+  return ext ? epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_F32, true>(c)
+             : epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_F32, false>(c);
+}
+
+template <bool kTplM>
+__device__ __forceinline__ bool epilogue_dispatch(EpiCtx& c, int method, bool fp64, bool ext) {
+  switch (method) {
+    case kSse:
+      return epilogue_m<kTplM, kSse>(c, fp64, ext);
+    case kSseNorm:
+      return epilogue_m<kTplM, kSseNorm>(c, fp64, ext);
+    case kCcorr:
+      return epilogue_m<kTplM, kCcorr>(c, fp64, ext);
+    default:
+      return epilogue_m<kTplM, kCcorrNorm>(c, fp64, ext);
+  }
+}
+
+template <bool kTplM>
 __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_constant__ ManyParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* sfull = reinterpret_cast<uint64_t*>(smem);   // [kStrips] strip built
@@ -147,8 +344,12 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  const uint32_t idesc = idesc_u8u8_s32(kM, p.NB);
+  const uint32_t idesc = kTplM ? idesc_u8u8_s32(128, kM) : idesc_u8u8_s32(kM, p.NB);
   const bool do_ext = p.ext != nullptr;
+  // templates as M: this lane's template and its running extremes keys
+  const uint32_t tl = ((uint32_t)(warp - kBuildWarps) & 3u) * 32 + lane;
+  const bool t_ok = tl < nt;
+  unsigned long long kmin = ~0ull, kmax = 0ull;
 
   uint32_t gx = 0;  // strips built / consumed so far (global x counter, same in all roles)
   bool ok = true;
@@ -233,8 +434,12 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
         atomicMax(p.err, p.tag);
       }
     } else if (warp == kMmaWarp) {
-      const bool leader = elect_one();
-      const uint32_t lbo_a = p.rows * 16, lbo_b = p.NB * 16;
+      // warp-uniform issue loop: descriptors advance by adding to their
+      // 16-byte-unit start-address field (shared addresses stay below 2^18)
+      const uint32_t lbo_s = p.rows * 16, lbo_t = p.NB * 16;
+      const uint32_t sstep = lbo_s >> 4, tstep = lbo_t >> 4;
+      const uint64_t tdesc0 = smem_desc_noswizzle(smem_u32(bmat), lbo_t, 128);
+      const uint32_t nk = p.kw / 32;
       for (uint32_t xi = 0; xi < nx; ++xi) {
         const uint32_t g = gx + xi, s = g % kStrips, d = g & 1u;
         const bool got_s = mbar_wait(&sfull[s], (g / kStrips) & 1u, deadline);
@@ -244,91 +449,42 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
           break;
         }
         tc_fence_after();
-        const uint32_t a0 = smem_u32(s_strip + s * strip_bytes);
-        const uint32_t b0 = smem_u32(bmat);
-        if (leader) {
-          uint32_t acc = 0;
-          for (uint32_t dy = 0; dy < p.h; ++dy)
-            for (uint32_t kk = 0; kk < p.kw / 32; ++kk) {
-              const uint64_t ad = smem_desc_noswizzle(a0 + (2 * kk) * lbo_a + dy * 16, lbo_a, 128);
-              const uint64_t bd = smem_desc_noswizzle(b0 + (dy * nch + 2 * kk) * lbo_b, lbo_b, 128);
-              asm volatile(
-                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + d * 128),
-                  "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                  : "memory");
-              acc = 1u;
-            }
-          mma_commit(&sempty[s]);
-          mma_commit(&dfull[d]);
+        const uint32_t dt = tmem + d * 128;
+        // one flat loop over template rows with running descriptors: the
+        // strip advances one 16-byte row per template row, the template block
+        // one row of nch chunks (a nested loop with computed descriptors
+        // issued at under half the tensor pipe's rate)
+        uint64_t sd = smem_desc_noswizzle(smem_u32(s_strip + s * strip_bytes), lbo_s, 128);
+        uint64_t td = tdesc0;
+        const uint64_t tdy = (uint64_t)(nch * tstep);
+        auto mma = [&](uint64_t tdk, uint64_t sdk, uint32_t acc) {
+          if constexpr (kTplM)
+            mma_i8_ss_warp(dt, tdk, sdk, idesc, acc);
+          else
+            mma_i8_ss_warp(dt, sdk, tdk, idesc, acc);
+        };
+        if (nk == 1) {
+          for (uint32_t dy = 0; dy < p.h; ++dy, sd += 1, td += tdy) mma(td, sd, dy != 0);
+        } else {  // two 32-byte K steps per template row (w in 33..64)
+          for (uint32_t dy = 0; dy < p.h; ++dy, sd += 1, td += tdy) {
+            mma(td, sd, dy != 0);
+            mma(td + 2 * tstep, sd + 2 * sstep, 1u);
+          }
         }
-        __syncwarp();
+        mma_commit_warp(&sempty[s]);
+        mma_commit_warp(&dfull[d]);
       }
       if (!ok && lane == 0) {
         *s_err = 1;
         atomicMax(p.err, p.tag);
       }
     } else {
-      // epilogue warps: quadrant q of the lanes (output rows), half of the templates
-      const uint32_t e = warp - kBuildWarps, q = e & 3, half = e >> 2;
-      const uint32_t m = q * 32 + lane, y = y0 + m;
-      const uint32_t ncol = p.NB / 2, c0 = half * ncol;
-      for (uint32_t xi = 0; xi < nx; ++xi) {
-        const uint32_t g = gx + xi, d = g & 1u;
-        if (!mbar_wait_sleep(&dfull[d], (g >> 1) & 1u, deadline)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t x = x0 + xi;
-        const uint32_t Y = s_y[xi * kM + m];
-        const bool row_ok = y < p.Ho;
-        float* orow = p.out ? p.out + ((size_t)y * p.Wo + x) * p.n + t0 : nullptr;
-        for (uint32_t cc = c0; cc < c0 + ncol; cc += 16) {
-          uint32_t v[16];
-          tmem_ld16(tmem_addr(tmem, q * 32, d * 128 + cc), v);
-          tmem_wait_ld();
-          float f[16];
-#pragma unroll
-          for (int k = 0; k < 16; ++k) f[k] = finish_score32(p.method, p.precision, v[k], Y, s_tss[cc + k]);
-          if (orow && row_ok) {
-            if (p.vec4 && cc + 16 <= nt) {
-#pragma unroll
-              for (int k = 0; k < 16; k += 4)
-                *reinterpret_cast<float4*>(orow + cc + k) = make_float4(f[k], f[k + 1], f[k + 2], f[k + 3]);
-            } else {
-              for (int k = 0; k < 16; ++k)
-                if (cc + k < nt) orow[cc + k] = f[k];
-            }
-          }
-          if (do_ext) {
-            // per template: smallest / largest value over this warp's 32 rows,
-            // the lowest row (= lowest linear index at this x) among ties
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              const uint32_t key = row_ok ? order_key(f[k]) : 0xFFFFFFFFu;
-              const uint32_t kmn = __reduce_min_sync(0xffffffffu, key);
-              const uint32_t ln = __ffs(__ballot_sync(0xffffffffu, key == kmn)) - 1;
-              const uint32_t keyx = row_ok ? order_key(f[k]) : 0u;
-              const uint32_t kmx = __reduce_max_sync(0xffffffffu, keyx);
-              const uint32_t lx = __ffs(__ballot_sync(0xffffffffu, keyx == kmx)) - 1;
-              if (lane == (uint32_t)k && cc + k < nt) {
-                const uint32_t ymn = y0 + q * 32 + ln, ymx = y0 + q * 32 + lx;
-                if (ymn < p.Ho) {
-                  const unsigned long long kn = ((unsigned long long)kmn << 32) | (ymn * p.Wo + x);
-                  atomicMin(&s_ext[2 * (cc + k)], kn);
-                }
-                if (ymx < p.Ho) {
-                  const unsigned long long kx = ((unsigned long long)kmx << 32) | (0xFFFFFFFFu - (ymx * p.Wo + x));
-                  atomicMax(&s_ext[2 * (cc + k) + 1], kx);
-                }
-              }
-            }
-          }
-        }
-        tc_fence_before();
-        mbar_arrive(&dempty[d]);
-      }
+      EpiCtx c{&p, tmem, dfull, dempty, s_y, s_tss, s_ext, reinterpret_cast<double*>(smem + p.ry_off),
+               gx, nx, x0, y0, t0, nt,
+               (uint32_t)(warp - kBuildWarps), (uint32_t)lane, deadline, kmin, kmax};
+      ok = epilogue_dispatch<kTplM>(c, p.method, p.precision == IPB_PRECISION_EXACT_FP64, do_ext);
+      kmin = c.kmin;
+      kmax = c.kmax;
       if (!ok) {
         *s_err = 1;
         atomicMax(p.err, p.tag);
@@ -337,8 +493,14 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
     gx += nx;
   }
 
+  if constexpr (kTplM) {
+    if (do_ext && warp >= kBuildWarps && warp < kMmaWarp && t_ok) {
+      atomicMin(&p.ext[2 * (t0 + tl)], kmin);
+      atomicMax(&p.ext[2 * (t0 + tl) + 1], kmax);
+    }
+  }
   __syncthreads();
-  if (do_ext)
+  if (!kTplM && do_ext)
     for (uint32_t t = threadIdx.x; t < nt; t += kThreads) {
       atomicMin(&p.ext[2 * (t0 + t)], s_ext[2 * t]);
       atomicMax(&p.ext[2 * (t0 + t) + 1], s_ext[2 * t + 1]);
@@ -389,6 +551,30 @@ __global__ void many_keys_finish_kernel(const unsigned long long* keys, uint32_t
   out[i] = r;
 }
 
+// Shared-memory carve for a template block of nb; returns the total bytes.
+uint32_t many_carve(ManyParams& p, uint32_t nb) {
+  uint32_t off = 1024;
+  p.b_off = off;
+  off += (uint32_t)align_up((size_t)p.h * p.kw * nb, 128);
+  p.tss_off = off;
+  off += (uint32_t)align_up(4 * nb, 128);
+  p.ext_off = off;
+  off += (uint32_t)align_up(16 * nb, 128);
+  p.img_off = off;
+  off += (uint32_t)align_up((size_t)p.rows * p.ip, 128);
+  p.strip_off = off;
+  off += (uint32_t)align_up((size_t)kStrips * (p.kw / 16) * p.rows * 16, 128);
+  p.y_off = off;
+  off += kXT * kM * 4;
+  p.v_off = off;
+  off += (uint32_t)align_up((size_t)p.rows * kXT * 4, 128);
+  p.ry_off = off;
+  off += kEpiWarps * (kM / 2) * 8;
+  return off;
+}
+
+constexpr uint32_t kSmemLimit = 227u * 1024u;
+
 }  // namespace
 
 cudaError_t launch_many_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s) {
@@ -427,28 +613,16 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   p.spatial = p.bands * p.xtiles;
   p.rows = kM + h - 1;
   p.ip = (uint32_t)align_up(kXT + p.kw + 16, 16);
-  // largest template block (multiple of 16, at most 128) whose carve fits
-  uint32_t off = 0;
+  // templates as M when a block of 128 fits and the bank fills most of it;
+  // otherwise the largest positions-as-M block (multiple of 16) that fits
+  uint32_t smem = many_carve(p, 128);
+  const bool tplm = smem <= kSmemLimit && n > 64;
   uint32_t nb = 128;
-  for (; nb >= 16; nb -= 16) {
-    off = 1024;
-    p.b_off = off;
-    off += (uint32_t)align_up((size_t)h * p.kw * nb, 128);
-    p.tss_off = off;
-    off += (uint32_t)align_up(4 * nb, 128);
-    p.ext_off = off;
-    off += (uint32_t)align_up(16 * nb, 128);
-    p.img_off = off;
-    off += (uint32_t)align_up((size_t)p.rows * p.ip, 128);
-    p.strip_off = off;
-    off += (uint32_t)align_up((size_t)kStrips * (p.kw / 16) * p.rows * 16, 128);
-    p.y_off = off;
-    off += kXT * kM * 4;
-    p.v_off = off;
-    off += (uint32_t)align_up((size_t)p.rows * kXT * 4, 128);
-    if (off <= 227u * 1024u) break;
+  if (!tplm) {
+    for (nb = std::min(112u, (n + 15) & ~15u); nb >= 16; nb -= 16)
+      if ((smem = many_carve(p, nb)) <= kSmemLimit) break;
+    if (nb < 16) return cudaErrorNotSupported;
   }
-  if (nb < 16) return cudaErrorNotSupported;
   p.NB = nb;
   p.nblocks = (n + nb - 1) / nb;
   p.method = method;
@@ -461,7 +635,11 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   p.tag = tag;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(many_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(many_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSmemLimit);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(many_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSmemLimit);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -471,7 +649,10 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   if (per > p.spatial) per = p.spatial;
   const uint32_t grid = per * p.nblocks;
   timer_begin(timer, kKernelMany, stream);
-  many_match_kernel<<<grid, kThreads, off, stream>>>(p);
+  if (tplm)
+    many_match_kernel<true><<<grid, kThreads, smem, stream>>>(p);
+  else
+    many_match_kernel<false><<<grid, kThreads, smem, stream>>>(p);
   count_launch(kKernelMany);
   timer_end(timer, stream);
   return cudaGetLastError();

@@ -183,6 +183,19 @@ __device__ __forceinline__ void mma_i8_ts_warp(uint32_t d_tmem, uint32_t a_tmem,
       : "memory");
 }
 
+// D[tmem] (+)= A[smem] * B[smem]^T issued by one elected lane of a converged
+// warp; `accumulate` = 0 overwrites D.
+__device__ __forceinline__ void mma_i8_ss_warp(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                               uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred e, acc;\n\t"
+      "setp.ne.b32 acc, %4, 0;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, acc;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // True in exactly one lane of a converged warp.
 __device__ __forceinline__ bool elect_one() {
   uint32_t pred = 0;

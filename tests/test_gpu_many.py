@@ -33,11 +33,17 @@ def _run(image, templates, method, precision=tm.Precision.ExactFp64, extremes=Tr
 
 CASES = [
     # (H, W), (n, h, w)
+    # positions as the MMA's M side (banks of at most 64, or large templates)
     ((300, 512), (40, 32, 32)),    # aligned image rows, n not a multiple of the block
     ((257, 333), (21, 24, 16)),    # odd sizes, n % 4 != 0 (scalar score stores)
     ((200, 260), (18, 48, 48)),    # smaller template blocks
     ((190, 300), (33, 64, 64)),
-    ((140, 150), (130, 8, 20)),    # more than one 128-template block
+    ((170, 200), (90, 40, 40)),    # a bank of 90 that does not fit as 128 templates
+    # templates as the MMA's M side (blocks of 128)
+    ((140, 150), (130, 8, 20)),    # two blocks, the second with 2 templates
+    ((260, 300), (100, 32, 32)),   # one partial block
+    ((190, 333), (70, 16, 16)),    # odd image width (no cp.async staging)
+    ((150, 200), (129, 36, 32)),   # the tallest template whose block fits
 ]
 
 
@@ -73,11 +79,12 @@ def test_many_templates_all_methods_and_f32_precision():
                 assert bits(out[:, :, t]).tolist() == bits(exp).tolist()
 
 
-def test_value_noise_workload_reduced():
+@pytest.mark.parametrize("n", [48, 160])
+def test_value_noise_workload_reduced(n):
     # the many-templates workload's generator at a reduced size
-    image, templates, locs = synthetic.value_noise_scene(W=512, H=384, n_templates=48, t=32, seed=4)
+    image, templates, locs = synthetic.value_noise_scene(W=512, H=384, n_templates=n, t=32, seed=4)
     out, ex = _run(image, templates, M.CrossCorrelationNormalized)
-    for t in range(0, 48, 5):
+    for t in range(0, n, 5):
         exp = O.match_exact(image, templates[t], M.CrossCorrelationNormalized, None, precision=0)
         assert bits(out[:, :, t]).tolist() == bits(exp).tolist()
         mx, mn, mxl, mnl = O.find_extremes(exp)
