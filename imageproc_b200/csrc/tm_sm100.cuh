@@ -183,21 +183,6 @@ __device__ __forceinline__ void mma_i8_ts_warp(uint32_t d_tmem, uint32_t a_tmem,
       : "memory");
 }
 
-// D[tmem] += A[tmem] * B[smem]^T issued by one elected lane of a converged
-// warp when `enable` is non-zero: the whole warp executes it, so a loop with
-// an optional MMA keeps uniform control flow.
-__device__ __forceinline__ void mma_i8_ts_warp_if(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
-                                                  uint32_t idesc, uint32_t enable) {
-  asm volatile(
-      "{\n\t.reg .pred e, p, acc;\n\t"
-      "setp.ne.b32 acc, 1, 0;\n\t"
-      "elect.sync _|e, 0xffffffff;\n\t"
-      "setp.ne.and.b32 p, %4, 0, e;\n\t"
-      "@p tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, acc;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(enable)
-      : "memory");
-}
-
 // D[tmem] (+)= A[smem] * B[smem]^T issued by one elected lane of a converged
 // warp; `accumulate` = 0 overwrites D.
 __device__ __forceinline__ void mma_i8_ss_warp(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,

@@ -438,6 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t kstride = 2u * q.zrows;  // one 32-byte K step of Z, in 16-byte units
       const uint32_t ksteps = q.kmma / 32;
       const uint32_t h = q.h;
+      const bool leader = elect_one();
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
         const bool got = mbar_wait(&full[s], (g / kStages) & 1u, deadline);
@@ -449,28 +450,33 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         const uint32_t r0 = st * L.rps, cnt = min(nrows, r0 + L.rps) - r0;
         const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
         // image row r feeds output rows n in [r-h+1, r] of the tile: the band
-        // [n0, n1) rounded out to 16 (rows past the map are computed, not
-        // stored). The whole warp runs one flat loop with uniform control
-        // flow; K steps past the template's width are disabled in the elect
-        // predicate rather than branched around.
-        uint32_t a = a_stage;
-        for (uint32_t r = r0; r < r0 + cnt; ++r, a += a_row_cols) {
+        // [n0, n1) rounded out to 16 (rows past the map are computed, not stored)
+#pragma unroll 4
+        for (uint32_t i = 0; i < kMaxRps; ++i) {
+          if (i >= cnt) break;
+          const uint32_t r = r0 + i;
           const uint32_t n0 = (r + 1 > h ? r + 1 - h : 0u) & ~15u;
           const uint32_t n1 = min(L.NT, (r & ~15u) + 16u);
           const uint32_t idesc = idesc0 | (((n1 - n0) >> 3) << 17);
           const uint32_t zrow = dlo + n0 + h + 15u - r;  // first Z row of the band
+          const uint32_t a = a_stage + i * a_row_cols;
+          if (leader) {
 #pragma unroll
-          for (int c = 0; c < NCORR; ++c) {
-            const uint32_t zo = zrow + (c == 0 ? 0u : zoff1);
+            for (int c = 0; c < NCORR; ++c) {
+              const uint32_t zo = zrow + (c == 0 ? 0u : zoff1);
 #pragma unroll
-            for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk)
-              mma_i8_ts_warp_if(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
-                                ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, kk < ksteps);
+              for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
+                if (kk < ksteps)
+                  mma_i8_ts(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                            ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
+              }
+            }
           }
         }
-        mma_commit_warp(&empty[s]);
+        if (leader) mma_commit(&empty[s]);
+        __syncwarp();
       }
-      if (ok) mma_commit_warp(dfull);
+      if (ok && leader) mma_commit(dfull);
       if (!ok && lane == 0) {
         *s_err = 1;
         atomicMax(L.err, L.tag);
