@@ -27,6 +27,13 @@ the data path, weak scaling.
              band of output rows.
 
 `--impl reference` times that CPU restatement alone as the reference arm.
+
+The line also carries `many_templates`: 512 templates of 32x32 against one
+4096x4096 value-noise scene (CrossCorrelationNormalized, exact sums, FP64
+normalisation), scored in one launch of the many-templates kernel with the
+position-major score maps (16.5M x 512 f32) and each template's
+find_extremes fused. `--only-many` runs that workload alone (with
+`--many-side` / `--many-templates` for smaller cases).
 """
 
 from __future__ import annotations
@@ -202,6 +209,71 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+MANY_T = 32
+
+
+def run_many(args, world, rank, local) -> dict:
+    """The many-templates workload; returns its summary (rank 0's view, time
+    = max over ranks)."""
+    import torch
+
+    from imageproc_b200 import _lib, device, synthetic
+
+    side, n = args.many_side, args.many_templates
+    image, templates, locs = synthetic.value_noise_scene(W=side, H=side, n_templates=n, t=MANY_T,
+                                                         seed=4 + rank)
+    dev = torch.device("cuda", local)
+    di = torch.from_numpy(image).to(dev)
+    dt = torch.from_numpy(templates).to(dev)
+    wo = side - MANY_T + 1
+    macs = wo * wo * MANY_T * MANY_T * n
+    out = torch.empty((wo, wo, n), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    method = 3  # CrossCorrelationNormalized
+
+    def query():
+        return device.match_templates_device(di, dt, method, extremes=True, out=out, stream=stream)
+
+    for _ in range(3):
+        flush.zero_()
+        query()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.many_steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.many_steps)]
+    barrier(world)
+    launches0 = _lib.launch_count()
+    ex = None
+    for k in range(args.many_steps):
+        flush.zero_()
+        starts[k].record(stream)
+        _, ex = query()  # the extremes come back to the host inside the step
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - launches0
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / args.many_steps, world)
+    hits = sum(1 for t in range(n) if ex[t].max_value_location == tuple(locs[t]))
+    pk = peaks()
+    out_bytes = 4.0 * wo * wo * n
+    hbm = out_bytes / (ms / 1e3) / 1e9
+    tens = 2.0 * macs / (ms / 1e3) / 1e12
+    del out
+    return {
+        "workload": (f"value_noise_scene {side}x{side} u8, {n} templates {MANY_T}x{MANY_T} (seeded "
+                     "crops + U{-6..6} noise), CrossCorrelationNormalized, position-major score maps "
+                     f"{wo}x{wo}x{n} f32 + fused find_extremes per template"),
+        "metric": METRIC, "value": world * macs / (ms / 1e3) / 1e9, "unit": UNIT,
+        "ms_per_query": ms, "templates_per_s": world * n / (ms / 1e3), "steps": args.many_steps,
+        "argmax_at_crop": f"{hits}/{n}", "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": hbm, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": hbm / pk["hbm_gbs"], "traffic": None,
+                     "note": (f"score-map writes {out_bytes / 1e9:.1f} GB per query; tensor side "
+                              f"{tens:.0f} of {2.0 * pk['bf16_tflops']:.0f} int8 TOP/s "
+                              f"(frac {tens / (2.0 * pk['bf16_tflops']):.3f})")},
+        "l2": "flushed between queries (256 MiB write)",
+    }
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -279,6 +351,8 @@ def run_ours(args, world, rank, local):
     h2d = len(VARIANTS) * (image.nbytes + template.nbytes) + 4 * mask.nbytes
     d2h = len(VARIANTS) * WO * HO * 4
 
+    del batch, plan
+    many = None if args.no_many else run_many(args, world, rank, local)
     if rank != 0:
         return
     pk = peaks()
@@ -333,6 +407,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "many_templates": many,
     }
     print(json.dumps(line), flush=True)
 
@@ -346,12 +421,21 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-many", action="store_true", help="skip the many-templates workload")
+    ap.add_argument("--only-many", action="store_true", help="run the many-templates workload alone")
+    ap.add_argument("--many-side", type=int, default=4096)
+    ap.add_argument("--many-templates", type=int, default=512)
+    ap.add_argument("--many-steps", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.only_many:
+            many = run_many(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(many), flush=True)
         else:
             run_ours(args, world, rank, local)
     finally:

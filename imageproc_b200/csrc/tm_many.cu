@@ -25,12 +25,13 @@
 //  * positions as M: A = the strip (M = 128 positions), B = NB templates
 //    (a multiple of 16, at most 112), for larger templates.
 //
-// Roles: 4 builder warps stage the image tile (cp.async), compute the window
-// sums Y = sum I^2 of every position of the tile, and build strips; one warp
-// issues the MMAs (warp-uniform loop, one elected lane); 8 epilogue warps
-// read the accumulator (double-buffered in tensor memory), apply the method,
-// write the scores and fold them into per-template extremes. Scores are
-// position-major: out[(y * Wo + x) * n_templates + t].
+// Roles: all warps stage each image tile (cp.async) and compute the window
+// sums Y = sum I^2 of its positions; then 2 builder warps build strips, one
+// warp issues the MMAs (one flat loop, one elected lane) and 16 epilogue
+// warps (four per tensor-memory lane quadrant) read the accumulator
+// (double-buffered in tensor memory), apply the method, write the scores and
+// fold them into per-template extremes. Scores are position-major:
+// out[(y * Wo + x) * n_templates + t].
 // Every wait is bounded (2 s) and reports through the error word.
 #include "tm_common.cuh"
 #include "tm_internal.h"
@@ -43,9 +44,11 @@ using namespace sm100;
 
 constexpr int kM = 128;           // output rows per tile
 constexpr int kXT = 32;           // output columns per tile
-constexpr int kBuildWarps = 4;
-constexpr int kEpiWarps = 8;
+constexpr int kBuildWarps = 2;
+constexpr int kEpiWarps = 16;  // four per lane quadrant: the epilogue is the longest role
 constexpr int kMmaWarp = kBuildWarps + kEpiWarps;
+constexpr int kEpiPerQuad = kEpiWarps / 4;      // epilogue warps per tensor-memory lane quadrant
+constexpr int kPosW = kM / kEpiPerQuad;         // templates as M: positions per epilogue warp
 constexpr int kThreads = (kMmaWarp + 1) * 32;
 constexpr int kStrips = 3;
 constexpr uint32_t kTmemCols = 256;  // two accumulators of up to 128 columns
@@ -91,9 +94,9 @@ struct EpiCtx {
   const uint32_t* s_y;
   const uint32_t* s_tss;
   unsigned long long* s_ext;
-  double* s_ry;  // [kEpiWarps][kM / 2] reciprocal roots of the strip's Y (templates as M)
+  double* s_ry;  // [kEpiWarps][kPosW] reciprocal roots of the strip's Y (templates as M)
   uint32_t gx, nx, x0, y0, t0, nt;
-  uint32_t e;  // epilogue warp index 0..7: lane quadrant e & 3, half e >> 2
+  uint32_t e;  // epilogue warp index: lane quadrant (e + kBuildWarps) & 3, share e >> 2
   uint32_t lane;
   unsigned long long deadline;
   unsigned long long kmin, kmax;  // templates as M: this lane's running extremes keys
@@ -105,19 +108,19 @@ struct EpiCtx {
 template <bool kTplM, int kMethod, int kPrec, bool kExt>
 __device__ __forceinline__ bool epilogue(EpiCtx& c) {
   const ManyParams& p = *c.p;
-  const uint32_t q = c.e & 3;
+  const uint32_t q = (c.e + kBuildWarps) & 3;  // = warp & 3, the lanes this warp may access
   if constexpr (kTplM) {
-    // lanes are templates; this warp takes half of the tile's 128 positions
-    const uint32_t mb = (c.e >> 2) * (kM / 2);
+    // lanes are templates; this warp takes kPosW of the tile's 128 positions
+    const uint32_t mb = (c.e >> 2) * kPosW;
     const uint32_t tl = q * 32 + c.lane;
     const bool t_ok = tl < c.nt;
     const uint32_t tss = c.s_tss[tl];
     // EXACT_FP64 normalisation: 1/sqrt(Y) once per position (shared by the
     // warp's 32 templates) and 1/sqrt(T) once per lane
     constexpr bool kNormW = method_is_norm(kMethod) && kPrec == IPB_PRECISION_EXACT_FP64;
-    double* s_ryw = c.s_ry + c.e * (kM / 2);
+    double* s_ryw = c.s_ry + c.e * kPosW;
     const double rT = (kNormW && tss) ? rsqrt_u32(tss) : 0.0;
-    const int mvalid = (int)p.Ho - (int)(c.y0 + mb);  // positions of the half inside the map
+    const int mvalid = (int)p.Ho - (int)(c.y0 + mb);  // positions of the share inside the map
     const size_t rstride = (size_t)p.Wo * p.n;
     for (uint32_t xi = 0; xi < c.nx; ++xi) {
       const uint32_t g = c.gx + xi, d = g & 1u;
@@ -129,13 +132,13 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
       const uint32_t idx0 = (c.y0 + mb) * p.Wo + x;
       if constexpr (kNormW) {
         __syncwarp();
-        for (uint32_t i = c.lane; i < (uint32_t)kM / 2; i += 32) {
+        for (uint32_t i = c.lane; i < (uint32_t)kPosW; i += 32) {
           const uint32_t yv = ycol[i];
           s_ryw[i] = yv ? rsqrt_u32(yv) : 0.0;
         }
         __syncwarp();
       }
-      for (int cc = 0; cc < kM / 2; cc += 16) {
+      for (int cc = 0; cc < kPosW; cc += 16) {
         uint32_t v[16];
         tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + mb + cc), v);
         uint32_t Y[16];
@@ -180,9 +183,9 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
     }
     return true;
   } else {
-    // lanes are positions (rows); this warp takes half of the block's templates
+    // lanes are positions (rows); the quadrant's warps take the block's
+    // 16-template chunks in turn
     const uint32_t m = q * 32 + c.lane, y = c.y0 + m;
-    const uint32_t ncol = p.NB / 2, c0 = (c.e >> 2) * ncol;
     const bool row_ok = y < p.Ho;
     for (uint32_t xi = 0; xi < c.nx; ++xi) {
       const uint32_t g = c.gx + xi, d = g & 1u;
@@ -191,7 +194,7 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
       const uint32_t x = c.x0 + xi;
       const uint32_t Y = c.s_y[xi * kM + m];
       float* orow = p.out ? p.out + ((size_t)y * p.Wo + x) * p.n + c.t0 : nullptr;
-      for (uint32_t cc = c0; cc < c0 + ncol; cc += 16) {
+      for (uint32_t cc = (c.e >> 2) * 16; cc < p.NB; cc += 16 * kEpiPerQuad) {
         uint32_t v[16];
         tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + cc), v);
         tmem_wait_ld();
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
   const uint32_t idesc = kTplM ? idesc_u8u8_s32(128, kM) : idesc_u8u8_s32(kM, p.NB);
   const bool do_ext = p.ext != nullptr;
   // templates as M: this lane's template and its running extremes keys
-  const uint32_t tl = ((uint32_t)(warp - kBuildWarps) & 3u) * 32 + lane;
+  const uint32_t tl = ((uint32_t)warp & 3u) * 32 + lane;
   const bool t_ok = tl < nt;
   unsigned long long kmin = ~0ull, kmax = 0ull;
 
@@ -569,7 +572,7 @@ uint32_t many_carve(ManyParams& p, uint32_t nb) {
   p.v_off = off;
   off += (uint32_t)align_up((size_t)p.rows * kXT * 4, 128);
   p.ry_off = off;
-  off += kEpiWarps * (kM / 2) * 8;
+  off += kEpiWarps * kPosW * 8;
   return off;
 }
 
