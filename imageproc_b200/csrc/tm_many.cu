@@ -138,6 +138,10 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
         }
         __syncwarp();
       }
+      // extremes of this strip: scores are never negative, so their f32 bits
+      // order like the values; positions come in increasing index order, so
+      // strict comparisons keep the first occurrence
+      uint32_t bmn = 0xFFFFFFFFu, jmn = 0, bmx = 0, jmx = 0;
       for (int cc = 0; cc < kPosW; cc += 16) {
         uint32_t v[16];
         tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + mb + cc), v);
@@ -161,11 +165,14 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
           }
           if (ocol) ocol[(size_t)(cc + k) * rstride] = f;
           if constexpr (kExt) {
-            if (t_ok) {
-              const unsigned long long key = (unsigned long long)order_key(f) << 32;
-              const uint32_t idx = idx0 + (uint32_t)(cc + k) * p.Wo;
-              c.kmin = min(c.kmin, key | idx);
-              c.kmax = max(c.kmax, key | (0xFFFFFFFFu - idx));
+            const uint32_t b = __float_as_uint(f);
+            if (b < bmn) {
+              bmn = b;
+              jmn = cc + k;
+            }
+            if (b > bmx) {
+              bmx = b;
+              jmx = cc + k;
             }
           }
         };
@@ -176,6 +183,15 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
 #pragma unroll
           for (int k = 0; k < 16; ++k)
             if (cc + k < mvalid) one(k);
+        }
+      }
+      if constexpr (kExt) {
+        // fold into the running keys (order_key of a non-negative f32 is its
+        // bits with the sign bit set); ties across strips go to the lower index
+        if (t_ok && mvalid > 0) {
+          const uint32_t imn = idx0 + jmn * p.Wo, imx = idx0 + jmx * p.Wo;
+          c.kmin = min(c.kmin, ((unsigned long long)(bmn | 0x80000000u) << 32) | imn);
+          c.kmax = max(c.kmax, ((unsigned long long)(bmx | 0x80000000u) << 32) | (0xFFFFFFFFu - imx));
         }
       }
       tc_fence_before();

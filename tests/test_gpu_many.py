@@ -67,6 +67,30 @@ def test_many_templates_bit_exact(case):
                 (float(mx), float(mn), mxl, mnl), (t, method)
 
 
+@pytest.mark.parametrize("n", [20, 100])  # positions as M, templates as M
+def test_many_templates_extremes_ties_first_occurrence(n):
+    # a periodic scene: every template's best (and worst) score repeats every
+    # 16 pixels, so the record must name the first occurrence in row-major order
+    g = np.random.default_rng(5)
+    tile = g.integers(0, 256, (16, 16), dtype=np.uint8)
+    image = np.tile(tile, (14, 20))
+    templates = np.stack([image[(t % 7):(t % 7) + 32, (t % 5):(t % 5) + 32] for t in range(n)])
+    for method in M:
+        out, ex = _run(image, templates, method)
+        for t in range(0, n, 7):
+            exp = O.match_exact(image, templates[t], method, None, precision=0)
+            assert bits(out[:, :, t]).tolist() == bits(exp).tolist()
+            mx, mn, mxl, mnl = O.find_extremes(exp)
+            e = ex[t]
+            assert (e.max_value, e.min_value, e.max_value_location, e.min_value_location) == \
+                (float(mx), float(mn), mxl, mnl), (t, method)
+    # an all-zero scene: every score ties (zero norm keeps the raw score, 0)
+    zero = np.zeros((120, 150), np.uint8)
+    out, ex = _run(zero, templates, M.CrossCorrelationNormalized)
+    assert not out.any()
+    assert all(e.max_value_location == (0, 0) and e.min_value_location == (0, 0) for e in ex)
+
+
 def test_many_templates_all_methods_and_f32_precision():
     g = np.random.default_rng(9)
     image = g.integers(0, 256, (180, 300), dtype=np.uint8)
