@@ -34,6 +34,13 @@ normalisation), scored in one launch of the many-templates kernel with the
 position-major score maps (16.5M x 512 f32) and each template's
 find_extremes fused. `--only-many` runs that workload alone (with
 `--many-side` / `--many-templates` for smaller cases).
+
+Two more objects cover the other exhaustive configurations: `small_map`
+(512x512 U{0..255} scene, 16x16 template, SumOfSquaredErrors: one map,
+device-resident and through the host API) and `batch_uneven` (256 uneven
+(image, template, method) pairs, image sides log-uniform in 256..4096,
+template sides 8..128, as one planned batch replayed as a CUDA graph with
+every map's find_extremes fused).
 """
 
 from __future__ import annotations
@@ -73,8 +80,9 @@ def peaks() -> dict:
 
 
 class ClockSampler:
-    """SM clock and throttle reasons sampled through NVML every 5 ms while the
-    timed region runs (read-only queries; nothing is set)."""
+    """SM clock and throttle reasons sampled through NVML every 2 ms while the
+    timed region runs, plus one sample as it starts and one as it ends
+    (read-only queries; nothing is set)."""
 
     REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
                "sw_power_cap": 0x4}
@@ -92,29 +100,35 @@ class ClockSampler:
             self._nvml = pynvml
             self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
             self._max = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._sample()
             self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
             self._nvml = None
         return self
 
-    def _run(self):
+    def _sample(self) -> bool:
         nv = self._nvml
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+            get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.samples.append((sm, self._max, get(self._h)))
+            return True
+        except Exception:
+            return False
+
+    def _run(self):
         while not self._stop.is_set():
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
-                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
-                rs = get(self._h)
-                self.samples.append((sm, self._max, rs))
-            except Exception:
+            if not self._sample():
                 return
-            time.sleep(0.005)
+            time.sleep(0.002)
 
     def __exit__(self, *exc):
         self._stop.set()
         if self._nvml:
             self.thread.join(timeout=2)
+            self._sample()
 
     def summary(self) -> dict | None:
         if not self.samples:
@@ -212,6 +226,12 @@ def run_reference(args, world, rank):
 MANY_T = 32
 
 
+def _traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+    tf = ROOT / "profiles" / "traffic.json"
+    return json.loads(tf.read_text()).get(kernel) if tf.exists() else None
+
+
 def run_many(args, world, rank, local) -> dict:
     """The many-templates workload; returns its summary (rank 0's view, time
     = max over ranks)."""
@@ -266,12 +286,82 @@ def run_many(args, world, rank, local) -> dict:
         "ms_per_query": ms, "templates_per_s": world * n / (ms / 1e3), "steps": args.many_steps,
         "argmax_at_crop": f"{hits}/{n}", "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": hbm, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                     "frac": hbm / pk["hbm_gbs"], "traffic": None,
+                     "frac": hbm / pk["hbm_gbs"], "traffic": _traffic("many_i8") if side == 4096 and n == 512
+                     else None,
                      "note": (f"score-map writes {out_bytes / 1e9:.1f} GB per query; tensor side "
                               f"{tens:.0f} of {2.0 * pk['bf16_tflops']:.0f} int8 TOP/s "
                               f"(frac {tens / (2.0 * pk['bf16_tflops']):.3f})")},
         "l2": "flushed between queries (256 MiB write)",
     }
+
+
+def _timed(fn, steps: int, flush, stream) -> float:
+    """Mean ms per call over `steps` calls, CUDA events on `stream`, L2
+    flushed before each call outside the events."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        fn()
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+
+
+def run_side_configs(args, world, rank, local) -> dict:
+    """The 512x512 single-map workload and the 256-pair uneven batch."""
+    import torch
+
+    from imageproc_b200 import device, synthetic
+    from imageproc_b200 import template_matching as tm
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    res = {}
+
+    image, template, _ = synthetic.uniform_scene(seed=0 + rank)
+    di, dt = torch.from_numpy(image).to(dev), torch.from_numpy(template).to(dev)
+    out = torch.empty((image.shape[0] - 15, image.shape[1] - 15), dtype=torch.float32, device=dev)
+    call = lambda: device.match_template_device(di, dt, 0, out=out, stream=stream)  # noqa: E731
+    for _ in range(3):
+        call()
+    ms = max_over_ranks(_timed(call, 20, flush, stream), world)
+    tm.match_template(image, template, 0)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        tm.match_template(image, template, 0)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) / 20 * 1e3, world)
+    macs = out.numel() * 16 * 16
+    res["small_map"] = {
+        "workload": "uniform_scene 512x512 U{0..255} u8, 16x16 seeded crop + U{-4..4}, "
+                    "SumOfSquaredErrors, 497x497 f32",
+        "value": world * macs / (ms / 1e3) / 1e9, "unit": UNIT, "us_per_map": ms * 1e3,
+        "e2e": {"value": world * macs / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "us_per_map": e2e_ms * 1e3,
+                "api": "match_template (numpy in, numpy out)"},
+    }
+
+    pairs = synthetic.uneven_pairs(seed=3 + rank)
+    items = [(torch.from_numpy(i).to(dev), torch.from_numpy(t).to(dev), m) for i, t, m in pairs]
+    batch = device.Batch(items, extremes=True)
+    plan = device.BatchPlan(batch, tm.Precision.ExactFp64)
+    info = plan.info()
+    for _ in range(3):
+        plan.launch(stream)
+    ms = max_over_ranks(_timed(lambda: plan.launch(stream), 5, flush, stream), world)
+    macs = sum((i.shape[0] - t.shape[0] + 1) * (i.shape[1] - t.shape[1] + 1) * t.size for i, t, _ in pairs)
+    res["batch_uneven"] = {
+        "workload": ("256 uneven pairs (uneven_pairs seed 3): image sides log-uniform 256..4096, "
+                     "template sides U{8..128}, U{0..255} content, methods U{0..3}, unmasked; "
+                     "score maps + fused find_extremes"),
+        "value": world * macs / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_batch": ms,
+        "pairs_per_s": world * len(pairs) / (ms / 1e3), "kernels_per_batch": info["kernels"],
+        "tensor_core_pairs": info["tensor_pairs"], "graph": True,
+    }
+    plan.close()
+    return res
 
 
 def run_ours(args, world, rank, local):
@@ -353,6 +443,7 @@ def run_ours(args, world, rank, local):
 
     del batch, plan
     many = None if args.no_many else run_many(args, world, rank, local)
+    side = {} if args.no_many else run_side_configs(args, world, rank, local)
     if rank != 0:
         return
     pk = peaks()
@@ -363,10 +454,7 @@ def run_ours(args, world, rank, local):
         per_launch_s = dom["total_ms"] / dom["launches"] / 1e3
         macs_per_launch = dom["algorithmic_macs"] / dom["launches"]
         achieved = 2.0 * macs_per_launch / per_launch_s / 1e12
-        traffic = None
-        tf = ROOT / "profiles" / "traffic.json"
-        if tf.exists():
-            traffic = json.loads(tf.read_text()).get(dom_name)
+        traffic = _traffic(dom_name)
         roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak_tops,
                     "unit": "TOP/s", "frac": achieved / int8_peak_tops, "traffic": traffic,
                     "kernel": dom_name, "launch_ms": per_launch_s * 1e3,
@@ -408,6 +496,7 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "many_templates": many,
+        **side,
     }
     print(json.dumps(line), flush=True)
 
