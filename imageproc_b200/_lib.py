@@ -8,6 +8,9 @@ and nothing else is ever substituted for it. A missing library raises
 from __future__ import annotations
 
 import ctypes as C
+import weakref
+
+import numpy as np
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libimageproc_b200.so"
@@ -144,8 +147,28 @@ def lib() -> C.CDLL:
         f = getattr(L, f"ipb_find_extremes_{suf}_device")
         f.argtypes = [C.c_void_p, u32, u32, C.POINTER(EXTREMES_STRUCTS[suf]), C.c_void_p]
         f.restype = C.c_int
+    L.ipb_host_alloc.argtypes = [C.c_size_t]
+    L.ipb_host_alloc.restype = C.c_void_p
+    L.ipb_host_free.argtypes = [C.c_void_p]
+    L.ipb_host_free.restype = None
     _lib = L
     return L
+
+
+def host_empty(shape, dtype=np.float32) -> np.ndarray:
+    """An uninitialised array in page-locked memory from the library's cache
+    (ipb_host_alloc), returned to the cache when the last view of it is gone;
+    ordinary memory when no CUDA device is usable. The device writes such
+    buffers at the full link rate, with no first-touch page faults."""
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) * dt.itemsize
+    L = lib()
+    p = L.ipb_host_alloc(n) if n else None
+    if not p:
+        return np.empty(shape, dt)
+    raw = (C.c_char * n).from_address(p)
+    weakref.finalize(raw, L.ipb_host_free, p)
+    return np.frombuffer(raw, dtype=dt).reshape(shape)
 
 
 def check(status: int) -> None:

@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdio>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <vector>
 #include <cstdlib>
@@ -393,6 +394,55 @@ using namespace ipb;
 IPB_API const char* ipb_last_error_message(void) { return g_last_error.c_str(); }
 
 IPB_API const char* ipb_version(void) { return "imageproc_b200 0.1.0 (sm_100a)"; }
+
+// ---- page-locked host buffers ---------------------------------------------------
+namespace {
+std::mutex g_host_mu;
+std::unordered_map<void*, size_t> g_host_live;  // pointer -> block size
+std::multimap<size_t, void*> g_host_free;        // cached blocks by size
+size_t g_host_cached = 0;
+constexpr size_t kHostCacheMax = size_t(1) << 30;
+}  // namespace
+
+IPB_API void* ipb_host_alloc(size_t bytes) {
+  const size_t sz = align_up(bytes ? bytes : 1, size_t(1) << 16);
+  {
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    auto it = g_host_free.lower_bound(sz);
+    if (it != g_host_free.end() && it->first <= 2 * sz) {  // reuse a block at most twice the size
+      void* p = it->second;
+      g_host_cached -= it->first;
+      g_host_live[p] = it->first;
+      g_host_free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, sz, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  g_host_live[p] = sz;
+  return p;
+}
+
+IPB_API void ipb_host_free(void* ptr) {
+  if (!ptr) return;
+  {
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    auto it = g_host_live.find(ptr);
+    if (it == g_host_live.end()) return;  // not a block of this cache
+    const size_t sz = it->second;
+    g_host_live.erase(it);
+    if (g_host_cached + sz <= kHostCacheMax) {
+      g_host_free.emplace(sz, ptr);
+      g_host_cached += sz;
+      return;
+    }
+  }
+  cudaFreeHost(ptr);
+}
 
 IPB_API uint64_t ipb_launch_count(void) { return g_launches.load(); }
 

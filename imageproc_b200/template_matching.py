@@ -110,12 +110,12 @@ def _run(fn_name: str, image, template, method, mask=None) -> np.ndarray:
         mask = _gray(mask, "mask")
         mh, mw = mask.shape
         valid = (mh, mw) == (h, w) and W >= w and H >= h
-        out = np.empty((H - h + 1, W - w + 1) if valid else (1, 1), np.float32)
+        out = _lib.host_empty((H - h + 1, W - w + 1) if valid else (1, 1))
         check(fn(_ptr(image, C.c_uint8), W, H, _ptr(template, C.c_uint8), w, h, int(m),
                  _ptr(mask, C.c_uint8), mw, mh, _ptr(out, C.c_float)))
         return out
     valid = W >= w and H >= h
-    out = np.empty((H - h + 1, W - w + 1) if valid else (1, 1), np.float32)
+    out = _lib.host_empty((H - h + 1, W - w + 1) if valid else (1, 1))
     check(fn(_ptr(image, C.c_uint8), W, H, _ptr(template, C.c_uint8), w, h, int(m),
              _ptr(out, C.c_float)))
     return out

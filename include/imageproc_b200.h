@@ -83,6 +83,15 @@ const char *ipb_last_error_message(void);
 /* Library version string. */
 const char *ipb_version(void);
 
+/* Page-locked host memory from a process-wide cache (additive API; no
+ * reference counterpart). Blocks freed with ipb_host_free are kept for reuse
+ * (up to 1 GiB in total), so a caller that allocates a score map per call
+ * gets memory that the device writes at the full link rate and that needs no
+ * first-touch page faults. Returns NULL when no CUDA device is usable; the
+ * entry points accept ordinary host memory as well. */
+void *ipb_host_alloc(size_t bytes);
+void ipb_host_free(void *ptr);
+
 /* Process-wide precision used by the reference-shaped entry points (the
  * ones without a precision argument). Default IPB_PRECISION_EXACT_FP64, or
  * the value of the environment variable IPB_PRECISION (0, 1, 2 or
