@@ -124,7 +124,7 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
     const size_t rstride = (size_t)p.Wo * p.n;
     for (uint32_t xi = 0; xi < c.nx; ++xi) {
       const uint32_t g = c.gx + xi, d = g & 1u;
-      if (!mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline)) return false;
+      if (!__all_sync(0xffffffffu, mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline))) return false;
       tc_fence_after();
       const uint32_t x = c.x0 + xi;
       const uint32_t* ycol = c.s_y + xi * kM + mb;
@@ -195,7 +195,8 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
         }
       }
       tc_fence_before();
-      mbar_arrive(&c.dempty[d]);
+      __syncwarp();
+      if (c.lane == 0) mbar_arrive(&c.dempty[d]);
     }
     return true;
   } else {
@@ -205,7 +206,7 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
     const bool row_ok = y < p.Ho;
     for (uint32_t xi = 0; xi < c.nx; ++xi) {
       const uint32_t g = c.gx + xi, d = g & 1u;
-      if (!mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline)) return false;
+      if (!__all_sync(0xffffffffu, mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline))) return false;
       tc_fence_after();
       const uint32_t x = c.x0 + xi;
       const uint32_t Y = c.s_y[xi * kM + m];
@@ -258,7 +259,8 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
         }
       }
       tc_fence_before();
-      mbar_arrive(&c.dempty[d]);
+      __syncwarp();
+      if (c.lane == 0) mbar_arrive(&c.dempty[d]);
     }
     return true;
   }
@@ -315,12 +317,12 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStrips; ++s) {
-      mbar_init(&sfull[s], kBuildWarps * 32);
+      mbar_init(&sfull[s], kBuildWarps);  // one arrive per builder warp
       mbar_init(&sempty[s], 1);
     }
     for (int d = 0; d < 2; ++d) {
       mbar_init(&dfull[d], 1);
-      mbar_init(&dempty[d], kEpiWarps * 32);
+      mbar_init(&dempty[d], kEpiWarps);   // one arrive per epilogue warp
     }
     mbar_init(drain, 1);
     *s_err = 0;
@@ -431,7 +433,8 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
       // strips: S_x[j][rho] = image row rho, bytes [xi + 16j, xi + 16j + 16)
       for (uint32_t xi = 0; xi < nx; ++xi) {
         const uint32_t g = gx + xi, s = g % kStrips;
-        if (g >= kStrips && !mbar_wait_sleep(&sempty[s], ((g / kStrips) + 1) & 1u, deadline)) {
+        const bool got = g < kStrips || mbar_wait_sleep(&sempty[s], ((g / kStrips) + 1) & 1u, deadline);
+        if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: the warp arrives as one below
           ok = false;
           break;
         }
@@ -446,7 +449,8 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
                          __byte_perm(w3, w4, sel));
         }
         fence_proxy_async_smem();
-        mbar_arrive(&sfull[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sfull[s]);
       }
       if (!ok) {
         *s_err = 1;

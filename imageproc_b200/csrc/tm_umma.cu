@@ -34,8 +34,10 @@
 // mask) whenever a CTA moves to a tile of another problem.
 //
 // Pipeline: image tiles are double-buffered in shared memory and loaded with
-// cp.async while the previous tile is computed. Builders fill 3 stages of RPS
-// A rows; one warp runs the MMA issue loop on warp-uniform values and one
+// cp.async while the previous tile is computed. Builders fill 2 stages of RPS
+// A rows (two large stages beat three smaller ones in the tensor memory left
+// beside the accumulators: each stage hand-off costs a tcgen05.wait::st and two
+// mbarrier round trips); one warp runs the MMA issue loop on warp-uniform values and one
 // elected lane issues the MMAs of a stage once it is full, then commits it
 // back to the builders; after the tile's last stage it commits the
 // accumulators to the epilogue (the builder warps), which reads them with
@@ -58,7 +60,7 @@ constexpr int kSubs = kBuilderWarps / 4;  // builder warps per tensor-memory lan
 constexpr int kBuilders = kBuilderWarps * 32;
 constexpr int kThreads = kBuilders + 32;
 constexpr int kWarps = kThreads / 32;
-constexpr int kStages = 3;
+constexpr int kStages = 2;  // A-row stages in tensor memory
 constexpr uint32_t kMaxRps = 16;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 2000000000ull;
@@ -141,8 +143,10 @@ __device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t
     for (int k = 0; k < CH; ++k) a[k] = __byte_perm(wv[k], wv[k + 1], sel);
     if constexpr (kRowSums) {
       if (c0 + CH <= (int)wq) {
+        uint32_t r4[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-        for (int k = 0; k < CH; ++k) rs = __dp4a(a[k], a[k], rs);
+        for (int k = 0; k < CH; ++k) r4[k & 3] = __dp4a(a[k], a[k], r4[k & 3]);
+        rs += (r4[0] + r4[1]) + (r4[2] + r4[3]);
       } else if (c0 <= (int)wq) {
 #pragma unroll
         for (int k = 0; k < CH; ++k) {
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], kBuilders);
+      mbar_init(&full[s], kBuilderWarps);  // one arrive per builder warp
       mbar_init(&empty[s], 1);
     }
     mbar_init(dfull, 1);
@@ -329,7 +333,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       }
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
-        if (g >= kStages && !mbar_wait_sleep(&empty[s], ((g / kStages) + 1) & 1u, deadline)) {
+        const bool got = g < kStages || mbar_wait_sleep(&empty[s], ((g / kStages) + 1) & 1u, deadline);
+        if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: the warp arrives as one below
           ok = false;
           break;
         }
@@ -349,7 +354,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         }
         tmem_wait_st();
         tc_fence_before();
-        mbar_arrive(&full[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
       }
       if (ok && !mbar_wait_sleep(dfull, tcount & 1u, deadline)) ok = false;
       // all builder threads reach this (every wait above is bounded): the row
