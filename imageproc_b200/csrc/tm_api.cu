@@ -91,7 +91,7 @@ void note_timed(KernelTimer* t, double macs, double bytes) {
 const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
-      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8"};
+      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -550,6 +550,151 @@ IPB_API ipb_status ipb_match_templates_device(const uint8_t* d_image, uint32_t W
   if (keys) IPB_CUDA(launch_many_keys_finish(keys, W - w + 1, d_extremes, n, s), "extremes finish");
   IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
   return IPB_OK;
+}
+
+// ---- integral images -------------------------------------------------------------
+namespace {
+ipb_status check_sat_args(uint32_t channels, int bits) {
+  if (channels != 1 && channels != 3 && channels != 4)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "channels must be 1 (Luma), 3 (Rgb) or 4 (Rgba)");
+  if (bits != 32 && bits != 64) return fail(IPB_ERR_INVALID_ARGUMENT, "integral images are u32 or u64");
+  return IPB_OK;
+}
+
+ipb_status host_sat(const uint8_t* image, uint32_t W, uint32_t H, uint32_t channels, bool squared, int bits,
+                    void* out) {
+  ipb_status st = check_sat_args(channels, bits);
+  if (st) return st;
+  const size_t ib = (size_t)W * H * channels;
+  const size_t ob = (size_t)(W + 1) * (H + 1) * channels * (bits / 8);
+  if ((!image && ib) || !out) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  if ((st = ensure(c, c->img, ib)) || (st = ensure(c, c->out, ob))) return st;
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  if (ib) IPB_CUDA(cudaMemcpyAsync(c->img.p, image, ib, cudaMemcpyHostToDevice, c->stream), "copy image");
+  IPB_CUDA(launch_sat(static_cast<const uint8_t*>(c->img.p), W, H, channels, squared, bits, c->out.p, c->stream),
+           "integral image launch");
+  IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy integral image");
+  return finish_sync(c, c->stream);
+}
+}  // namespace
+
+IPB_API ipb_status ipb_integral_image_u32(const uint8_t* image, uint32_t W, uint32_t H, uint32_t channels,
+                                          uint32_t* out) {
+  return host_sat(image, W, H, channels, false, 32, out);
+}
+IPB_API ipb_status ipb_integral_squared_image_u32(const uint8_t* image, uint32_t W, uint32_t H,
+                                                  uint32_t channels, uint32_t* out) {
+  return host_sat(image, W, H, channels, true, 32, out);
+}
+IPB_API ipb_status ipb_integral_image_u64(const uint8_t* image, uint32_t W, uint32_t H, uint32_t channels,
+                                          uint64_t* out) {
+  return host_sat(image, W, H, channels, false, 64, out);
+}
+IPB_API ipb_status ipb_integral_squared_image_u64(const uint8_t* image, uint32_t W, uint32_t H,
+                                                  uint32_t channels, uint64_t* out) {
+  return host_sat(image, W, H, channels, true, 64, out);
+}
+IPB_API ipb_status ipb_integral_image_device(const uint8_t* d_image, uint32_t W, uint32_t H, uint32_t channels,
+                                             int squared, int bits, void* d_out, void* stream) {
+  ipb_status st = check_sat_args(channels, bits);
+  if (st) return st;
+  if ((!d_image && (size_t)W * H) || !d_out) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  IPB_CUDA(launch_sat(d_image, W, H, channels, squared != 0, bits, d_out, static_cast<cudaStream_t>(stream)),
+           "integral image launch");
+  return IPB_OK;
+}
+
+// ---- non-maximum suppression ------------------------------------------------------
+namespace {
+ipb_status host_suppress(int type, size_t esize, const void* image, uint32_t W, uint32_t H, uint32_t radius,
+                         void* out) {
+  const size_t bytes = (size_t)W * H * esize;
+  if ((!image && bytes) || (!out && bytes)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!bytes) return IPB_OK;  // empty image: empty output
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  if ((st = ensure(c, c->img, bytes)) || (st = ensure(c, c->out, bytes)) ||
+      (st = ensure(c, c->scratch, (size_t)W * H * 4)))
+    return st;
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(cudaMemcpyAsync(c->img.p, image, bytes, cudaMemcpyHostToDevice, c->stream), "copy image");
+  IPB_CUDA(launch_suppress(type, c->img.p, W, H, radius, c->out.p, static_cast<uint32_t*>(c->scratch.p), c->stream),
+           "suppress_non_maximum launch");
+  IPB_CUDA(cudaMemcpyAsync(out, c->out.p, bytes, cudaMemcpyDeviceToHost, c->stream), "copy output");
+  return finish_sync(c, c->stream);
+}
+
+ipb_status device_suppress(int type, const void* d_image, uint32_t W, uint32_t H, uint32_t radius, void* d_out,
+                           void* stream) {
+  if (((size_t)W * H) && (!d_image || !d_out)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!((size_t)W * H)) return IPB_OK;
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  if ((st = ensure(c, c->scratch, (size_t)W * H * 4))) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  IPB_CUDA(cudaStreamWaitEvent(s, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(launch_suppress(type, d_image, W, H, radius, d_out, static_cast<uint32_t*>(c->scratch.p), s),
+           "suppress_non_maximum launch");
+  IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
+  return IPB_OK;
+}
+}  // namespace
+
+#define IPB_DEFINE_SUPPRESS(T, S, CODE)                                                                  \
+  IPB_API ipb_status ipb_suppress_non_maximum_##S(const T* image, uint32_t W, uint32_t H, uint32_t radius, \
+                                                  T* out) {                                             \
+    return host_suppress(CODE, sizeof(T), image, W, H, radius, out);                                     \
+  }                                                                                                     \
+  IPB_API ipb_status ipb_suppress_non_maximum_##S##_device(const T* d_image, uint32_t W, uint32_t H,      \
+                                                           uint32_t radius, T* d_out, void* stream) {   \
+    return device_suppress(CODE, d_image, W, H, radius, d_out, stream);                                  \
+  }
+IPB_DEFINE_SUPPRESS(uint8_t, u8, IPB_TYPE_U8)
+IPB_DEFINE_SUPPRESS(uint16_t, u16, IPB_TYPE_U16)
+IPB_DEFINE_SUPPRESS(uint32_t, u32, IPB_TYPE_U32)
+IPB_DEFINE_SUPPRESS(uint64_t, u64, IPB_TYPE_U64)
+IPB_DEFINE_SUPPRESS(int8_t, i8, IPB_TYPE_I8)
+IPB_DEFINE_SUPPRESS(int16_t, i16, IPB_TYPE_I16)
+IPB_DEFINE_SUPPRESS(int32_t, i32, IPB_TYPE_I32)
+IPB_DEFINE_SUPPRESS(int64_t, i64, IPB_TYPE_I64)
+IPB_DEFINE_SUPPRESS(float, f32, IPB_TYPE_F32)
+#undef IPB_DEFINE_SUPPRESS
+
+IPB_API ipb_status ipb_local_maxima(const uint32_t* xs, const uint32_t* ys, const float* scores, uint32_t n,
+                                    uint32_t radius, uint32_t* out_indices, uint32_t* out_count) {
+  if (!out_count || (n && (!xs || !ys || !scores || !out_indices)))
+    return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  *out_count = 0;
+  if (n == 0) return IPB_OK;
+  uint32_t max_y = 0;  // sizes the row table; the kernels find the rows themselves
+  for (uint32_t i = 0; i < n; ++i) max_y = ys[i] > max_y ? ys[i] : max_y;
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  const size_t nb = (size_t)n * 4;
+  const size_t sb = local_maxima_scratch_bytes(n, max_y);
+  if ((st = ensure(c, c->img, 4 * nb + 256)) || (st = ensure(c, c->scratch, sb))) return st;
+  uint8_t* d = static_cast<uint8_t*>(c->img.p);
+  uint32_t* d_xs = reinterpret_cast<uint32_t*>(d);
+  uint32_t* d_ys = reinterpret_cast<uint32_t*>(d + nb);
+  float* d_sc = reinterpret_cast<float*>(d + 2 * nb);
+  uint32_t* d_out = reinterpret_cast<uint32_t*>(d + 3 * nb);
+  uint32_t* d_count = reinterpret_cast<uint32_t*>(d + 4 * nb);
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(cudaMemcpyAsync(d_xs, xs, nb, cudaMemcpyHostToDevice, c->stream), "copy xs");
+  IPB_CUDA(cudaMemcpyAsync(d_ys, ys, nb, cudaMemcpyHostToDevice, c->stream), "copy ys");
+  IPB_CUDA(cudaMemcpyAsync(d_sc, scores, nb, cudaMemcpyHostToDevice, c->stream), "copy scores");
+  IPB_CUDA(launch_local_maxima(d_xs, d_ys, d_sc, n, radius, max_y, c->scratch.p, sb, d_out, d_count, c->stream),
+           "local_maxima launch");
+  IPB_CUDA(cudaMemcpyAsync(out_count, d_count, 4, cudaMemcpyDeviceToHost, c->stream), "copy count");
+  IPB_CUDA(cudaMemcpyAsync(out_indices, d_out, nb, cudaMemcpyDeviceToHost, c->stream), "copy indices");
+  return finish_sync(c, c->stream);
 }
 
 IPB_API ipb_status ipb_match_template_device(const uint8_t* d_image, uint32_t W, uint32_t H,

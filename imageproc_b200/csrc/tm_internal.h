@@ -21,6 +21,7 @@ enum KernelId : int {
   kKernelExtremes,
   kKernelUmma,
   kKernelMany,
+  kKernelSuppress,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -83,6 +84,28 @@ cudaError_t launch_integral_squared(const uint8_t* img, uint32_t W, uint32_t H,
                                     unsigned long long* sat, cudaStream_t s);
 cudaError_t launch_integral(const uint8_t* img, uint32_t W, uint32_t H,
                             unsigned long long* sat, cudaStream_t s);
+
+// ---- integral-image API (tm_sat.cu) -----------------------------------------
+// (W+1) x (H+1) x channels table of u32 (bits = 32, wrapping) or u64 sums of
+// F or F^2, channels 1, 3 or 4 interleaved (src/integral_image.rs:50, :89).
+cudaError_t launch_sat(const uint8_t* img, uint32_t W, uint32_t H, uint32_t channels, bool squared, int bits,
+                       void* sat, cudaStream_t s);
+
+// ---- non-maximum suppression (tm_suppress.cu) -------------------------------
+enum ElemType : int {
+  IPB_TYPE_U8 = 0, IPB_TYPE_U16, IPB_TYPE_U32, IPB_TYPE_U64,
+  IPB_TYPE_I8, IPB_TYPE_I16, IPB_TYPE_I32, IPB_TYPE_I64, IPB_TYPE_F32
+};
+// suppress_non_maximum of a W x H image of `type`; bx = W*H u32 scratch.
+cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
+                            cudaStream_t s);
+size_t local_maxima_scratch_bytes(uint32_t n, uint32_t max_y);
+// local_maxima of n device points (max_y = the largest y): writes the kept
+// points' input indices in the reference's order to out and their number to
+// *count (both device memory).
+cudaError_t launch_local_maxima(const uint32_t* xs, const uint32_t* ys, const float* scores, uint32_t n,
+                                uint32_t radius, uint32_t max_y, void* scratch, size_t scratch_bytes,
+                                uint32_t* out, uint32_t* count, cudaStream_t s);
 
 // ---- CUDA-core exact kernel (tm_exact_cc.cu) ------------------------------
 size_t exact_cc_scratch_bytes(const MatchArgs& a);

@@ -1,0 +1,292 @@
+// tm_suppress.cu -- imageproc's non-maximum suppression on the device
+// (src/suppress.rs).
+//
+// suppress_non_maximum (:10-107) keeps a pixel's value when it is the
+// greatest in the (2r+1) x (2r+1) window centred on it (clipped to the image)
+// and writes zero elsewhere; among equal values the pixel with the
+// lexicographically smaller (x, y) wins. The reference finds this with a grid
+// of (r+1)-cells; the kept set is exactly the per-pixel rule (its own tests
+// check that against a naive implementation, :274-318), which is separable:
+// "greatest" is the maximum under the total order (value, then (x, y)
+// reversed), and the window maximum of a rectangle is the column maximum of
+// row maxima. So:
+//   row pass:    for every pixel, the column x' in [x-r, x+r] holding the row
+//                window's winner (largest value, smallest x' among equals);
+//   column pass: for every pixel, the winner of the column window over
+//                those row winners (largest value, then smallest (x', y'));
+//                the pixel keeps its value iff it is that winner.
+// Values compare through order-preserving u64 keys, so one kernel serves
+// every integer type (and f32 score maps, where NaN compares above numbers).
+//
+// local_maxima (:111-173) works on a list of scored points: stable sort by
+// (y, x) (CUB radix sort), per-row start offsets, then one thread per point
+// runs the reference's scan over the rows of its window -- including the
+// reference's upper bound, which stops one row short of the last occupied
+// row when the window reaches it -- and the kept points are compacted in
+// sorted order.
+#include <algorithm>
+#include <type_traits>
+
+#include <cub/cub.cuh>
+
+#include "tm_common.cuh"
+#include "tm_internal.h"
+
+namespace ipb {
+namespace {
+
+template <typename T>
+__device__ __forceinline__ unsigned long long okey(T v) {
+  if constexpr (std::is_same<T, float>::value) {
+    const uint32_t b = __float_as_uint(v);
+    return (b & 0x80000000u) ? (unsigned long long)(~b) : (unsigned long long)(b | 0x80000000u);
+  } else if constexpr (std::is_signed<T>::value) {
+    return (unsigned long long)(long long)v ^ 0x8000000000000000ull;
+  } else {
+    return (unsigned long long)v;
+  }
+}
+
+constexpr int kRowThreads = 256;
+
+// Row pass: best column of the row window of every pixel, into `bx`.
+template <typename T>
+__global__ void __launch_bounds__(kRowThreads) snm_rows_kernel(const T* __restrict__ img, uint32_t W, uint32_t H,
+                                                               uint32_t r, uint32_t* __restrict__ bx) {
+  extern __shared__ unsigned long long s_key[];  // [kRowThreads + 2r] keys of the segment and its halo
+  const uint32_t xs = blockIdx.x * kRowThreads;  // first pixel of the segment
+  const uint32_t lo = xs > r ? xs - r : 0u;
+  const uint32_t hi = (uint32_t)min((unsigned long long)W, (unsigned long long)xs + kRowThreads + r);
+  const uint32_t x = xs + threadIdx.x;
+  for (uint32_t y = blockIdx.y; y < H; y += gridDim.y) {
+    const T* row = img + (size_t)y * W;
+    __syncthreads();  // the previous row's keys are no longer read
+    for (uint32_t c = lo + threadIdx.x; c < hi; c += kRowThreads) s_key[c - lo] = okey(row[c]);
+    __syncthreads();
+    if (x < W) {
+      const uint32_t a = x > r ? x - r : 0u;
+      const uint32_t b = (uint32_t)min((unsigned long long)W - 1, (unsigned long long)x + r);
+      uint32_t best = a;
+      unsigned long long bk = s_key[a - lo];
+      for (uint32_t c = a + 1; c <= b; ++c) {
+        const unsigned long long k = s_key[c - lo];
+        if (k > bk) {  // strictly greater: the smaller column wins among equals
+          bk = k;
+          best = c;
+        }
+      }
+      bx[(size_t)y * W + x] = best;
+    }
+  }
+}
+
+// Row pass for windows wider than shared memory holds: the same scan from
+// global memory.
+template <typename T>
+__global__ void __launch_bounds__(kRowThreads) snm_rows_global_kernel(const T* __restrict__ img, uint32_t W,
+                                                                      uint32_t H, uint32_t r,
+                                                                      uint32_t* __restrict__ bx) {
+  const uint32_t x = blockIdx.x * kRowThreads + threadIdx.x;
+  if (x >= W) return;
+  for (uint32_t y = blockIdx.y; y < H; y += gridDim.y) {
+    const T* row = img + (size_t)y * W;
+    const uint32_t a = x > r ? x - r : 0u;
+    const uint32_t b = (uint32_t)min((unsigned long long)W - 1, (unsigned long long)x + r);
+    uint32_t best = a;
+    unsigned long long bk = okey(row[a]);
+    for (uint32_t c = a + 1; c <= b; ++c) {
+      const unsigned long long k = okey(row[c]);
+      if (k > bk) {
+        bk = k;
+        best = c;
+      }
+    }
+    bx[(size_t)y * W + x] = best;
+  }
+}
+
+// Column pass: winner of the column window over the row winners; the pixel
+// keeps its value iff it is the winner. Ties go to the smaller x, then the
+// smaller y (the reference's tuple order (x, y)).
+template <typename T>
+__global__ void __launch_bounds__(256) snm_cols_kernel(const T* __restrict__ img, uint32_t W, uint32_t H, uint32_t r,
+                                                       const uint32_t* __restrict__ bx, T* __restrict__ out) {
+  const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
+  const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (x >= W || y >= H) return;
+  const uint32_t a = y > r ? y - r : 0u;
+  const uint32_t b = (uint32_t)min((unsigned long long)H - 1, (unsigned long long)y + r);
+  uint32_t wx = bx[(size_t)a * W + x], wy = a;
+  unsigned long long wk = okey(img[(size_t)a * W + wx]);
+  for (uint32_t yy = a + 1; yy <= b; ++yy) {
+    const uint32_t cx = bx[(size_t)yy * W + x];
+    const unsigned long long k = okey(img[(size_t)yy * W + cx]);
+    if (k > wk || (k == wk && cx < wx)) {  // equal x: the earlier row already holds
+      wk = k;
+      wx = cx;
+      wy = yy;
+    }
+  }
+  const T v = img[(size_t)y * W + x];
+  out[(size_t)y * W + x] = (wx == x && wy == y) ? v : T(0);
+}
+
+template <typename T>
+cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, uint32_t* bx, cudaStream_t s) {
+  if (W == 0 || H == 0) return cudaSuccess;
+  const dim3 rg((W + kRowThreads - 1) / kRowThreads, H < 65535u ? H : 65535u);
+  const size_t halo = (size_t)kRowThreads + 2 * (size_t)r;
+  if (halo * sizeof(unsigned long long) <= 48 * 1024)
+    snm_rows_kernel<T><<<rg, kRowThreads, halo * sizeof(unsigned long long), s>>>(img, W, H, r, bx);
+  else
+    snm_rows_global_kernel<T><<<rg, kRowThreads, 0, s>>>(img, W, H, r, bx);
+  count_launch(kKernelSuppress);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((H + 7) / 8 > 65535u) return cudaErrorInvalidValue;  // images up to 524280 rows
+  snm_cols_kernel<T><<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, s>>>(img, W, H, r, bx, out);
+  count_launch(kKernelSuppress);
+  return cudaGetLastError();
+}
+
+// ---- local_maxima ------------------------------------------------------------
+
+__global__ void lm_keys_kernel(const uint32_t* xs, const uint32_t* ys, uint32_t n, unsigned long long* keys,
+                               uint32_t* idx) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    keys[i] = ((unsigned long long)ys[i] << 32) | xs[i];
+    idx[i] = i;
+  }
+}
+
+// row_start[y] = first sorted position with row >= y, for y = 0 .. height + 1
+__global__ void lm_rows_kernel(const unsigned long long* skeys, uint32_t n, uint32_t* row_start, uint32_t rows) {
+  const uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= rows) return;
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) / 2;
+    if ((uint32_t)(skeys[mid] >> 32) < y) lo = mid + 1;
+    else hi = mid;
+  }
+  row_start[y] = lo;
+}
+
+__global__ void lm_flags_kernel(const unsigned long long* skeys, const uint32_t* sidx, const float* scores,
+                                uint32_t n, uint32_t radius, uint32_t height, const uint32_t* row_start,
+                                uint32_t* flags) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t cy = (uint32_t)(skeys[i] >> 32), cx = (uint32_t)skeys[i];
+  const float cs = scores[sidx[i]];
+  // u32 arithmetic as in the reference (release builds wrap)
+  const uint32_t row_lower = cy > radius ? cy - radius : 0u;
+  const uint32_t row_upper = (uint32_t)(cy + radius + 1u) > height ? height : (uint32_t)(cy + radius + 1u);
+  uint32_t is_max = 1;
+  for (uint32_t y = row_lower; y < row_upper && is_max; ++y)
+    for (uint32_t k = row_start[y]; k < row_start[y + 1]; ++k) {
+      const uint32_t x = (uint32_t)skeys[k];
+      if ((uint32_t)(x + radius) < cx) continue;
+      if (x > (uint32_t)(cx + radius)) break;
+      const float s = scores[sidx[k]];
+      if (s > cs) {
+        is_max = 0;
+        break;
+      }
+      if (s < cs) continue;
+      if (y < cy || (y == cy && x < cx)) {  // (c.y, c.x) < (cy, cx)
+        is_max = 0;
+        break;
+      }
+    }
+  flags[i] = is_max;
+}
+
+__global__ void lm_compact_kernel(const uint32_t* flags, const uint32_t* pos, const uint32_t* sidx, uint32_t n,
+                                  uint32_t* out, uint32_t* count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flags[i]) out[pos[i]] = sidx[i];
+  if (i == n - 1) *count = pos[i] + flags[i];
+}
+
+}  // namespace
+
+cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
+                            cudaStream_t s) {
+  switch (type) {
+    case IPB_TYPE_U8: return launch_snm_t(static_cast<const uint8_t*>(img), W, H, r, static_cast<uint8_t*>(out), bx, s);
+    case IPB_TYPE_U16:
+      return launch_snm_t(static_cast<const uint16_t*>(img), W, H, r, static_cast<uint16_t*>(out), bx, s);
+    case IPB_TYPE_U32:
+      return launch_snm_t(static_cast<const uint32_t*>(img), W, H, r, static_cast<uint32_t*>(out), bx, s);
+    case IPB_TYPE_U64:
+      return launch_snm_t(static_cast<const unsigned long long*>(img), W, H, r,
+                          static_cast<unsigned long long*>(out), bx, s);
+    case IPB_TYPE_I8: return launch_snm_t(static_cast<const int8_t*>(img), W, H, r, static_cast<int8_t*>(out), bx, s);
+    case IPB_TYPE_I16:
+      return launch_snm_t(static_cast<const int16_t*>(img), W, H, r, static_cast<int16_t*>(out), bx, s);
+    case IPB_TYPE_I32:
+      return launch_snm_t(static_cast<const int32_t*>(img), W, H, r, static_cast<int32_t*>(out), bx, s);
+    case IPB_TYPE_I64:
+      return launch_snm_t(static_cast<const long long*>(img), W, H, r, static_cast<long long*>(out), bx, s);
+    case IPB_TYPE_F32: return launch_snm_t(static_cast<const float*>(img), W, H, r, static_cast<float*>(out), bx, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+size_t local_maxima_scratch_bytes(uint32_t n, uint32_t max_y) {
+  size_t sort_tmp = 0, scan_tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (const unsigned long long*)nullptr,
+                                  (unsigned long long*)nullptr, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (int)n);
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)n);
+  const size_t per = align_up((size_t)n * 8, 256);
+  const size_t per4 = align_up((size_t)n * 4, 256);
+  return 2 * per + 5 * per4 + align_up(((size_t)max_y + 2) * 4, 256) + align_up(std::max(sort_tmp, scan_tmp), 256) +
+         256;
+}
+
+// Inputs on the device; out (n indices) and count on the device.
+cudaError_t launch_local_maxima(const uint32_t* xs, const uint32_t* ys, const float* scores, uint32_t n,
+                                uint32_t radius, uint32_t max_y, void* scratch, size_t scratch_bytes,
+                                uint32_t* out, uint32_t* count, cudaStream_t s) {
+  if (n == 0) return cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+  uint8_t* p = static_cast<uint8_t*>(scratch);
+  auto take = [&](size_t bytes) {
+    void* q = p;
+    p += align_up(bytes, 256);
+    return q;
+  };
+  auto* keys = static_cast<unsigned long long*>(take((size_t)n * 8));
+  auto* skeys = static_cast<unsigned long long*>(take((size_t)n * 8));
+  auto* idx = static_cast<uint32_t*>(take((size_t)n * 4));
+  auto* sidx = static_cast<uint32_t*>(take((size_t)n * 4));
+  auto* flags = static_cast<uint32_t*>(take((size_t)n * 4));
+  auto* pos = static_cast<uint32_t*>(take((size_t)n * 4));
+  take((size_t)n * 4);
+  auto* row_start = static_cast<uint32_t*>(take(((size_t)max_y + 2) * 4));
+  void* tmp = p;
+  size_t tmp_bytes = scratch_bytes - (size_t)(p - static_cast<uint8_t*>(scratch));
+  const uint32_t blocks = (n + 255) / 256;
+  lm_keys_kernel<<<blocks, 256, 0, s>>>(xs, ys, n, keys, idx);
+  count_launch(kKernelSuppress);
+  // radix sort is stable: equal (y, x) keep their input order
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, skeys, idx, sidx, (int)n, 0, 64, s);
+  if (e != cudaSuccess) return e;
+  // rows 0 .. max_y + 1 (max_y bounds every y, so row_start covers the
+  // height the reference takes from the last sorted point)
+  lm_rows_kernel<<<(max_y + 2 + 255) / 256, 256, 0, s>>>(skeys, n, row_start, max_y + 2);
+  count_launch(kKernelSuppress);
+  // height = the largest y: the last sorted key's row, read on the device
+  lm_flags_kernel<<<blocks, 256, 0, s>>>(skeys, sidx, scores, n, radius, max_y, row_start, flags);
+  count_launch(kKernelSuppress);
+  e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, flags, pos, (int)n, s);
+  if (e != cudaSuccess) return e;
+  lm_compact_kernel<<<blocks, 256, 0, s>>>(flags, pos, sidx, n, out, count);
+  count_launch(kKernelSuppress);
+  return cudaGetLastError();
+}
+
+}  // namespace ipb

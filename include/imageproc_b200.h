@@ -310,6 +310,63 @@ IPB_DECLARE_FIND_EXTREMES(int64_t, i64)
 IPB_DECLARE_FIND_EXTREMES(float, f32)
 IPB_DECLARE_FIND_EXTREMES(double, f64)
 
+/* ---- integral images ---------------------------------------------------------
+ * integral_image / integral_squared_image (src/integral_image.rs:50, :89,
+ * implementation :98-153) of a u8 image with `channels` interleaved channels
+ * (1 = Luma, 3 = Rgb, 4 = Rgba): a (width + 1) x (height + 1) table, row-major,
+ * `channels` values per entry, entry (x, y) = sum of F(x', y') (or F(x', y')^2)
+ * over x' < x, y' < y, so the top row and the left column are zero. The u32
+ * forms wrap modulo 2^32 like the reference's u32 sums in a release build; the
+ * u64 forms are exact. An empty image gives a table of zeros.
+ * sum_image_pixels and variance (:250, :303) are O(1) lookups into these
+ * tables and live in the C++ and Python mirrors. */
+ipb_status ipb_integral_image_u32(const uint8_t *image, uint32_t width, uint32_t height,
+                                  uint32_t channels, uint32_t *out);
+ipb_status ipb_integral_squared_image_u32(const uint8_t *image, uint32_t width, uint32_t height,
+                                          uint32_t channels, uint32_t *out);
+ipb_status ipb_integral_image_u64(const uint8_t *image, uint32_t width, uint32_t height,
+                                  uint32_t channels, uint64_t *out);
+ipb_status ipb_integral_squared_image_u64(const uint8_t *image, uint32_t width, uint32_t height,
+                                          uint32_t channels, uint64_t *out);
+/* The same on device buffers, enqueued on `stream`; bits = 32 or 64. */
+ipb_status ipb_integral_image_device(const uint8_t *d_image, uint32_t width, uint32_t height,
+                                     uint32_t channels, int squared, int bits, void *d_out,
+                                     void *stream);
+
+/* ---- non-maximum suppression ---------------------------------------------------
+ * suppress_non_maximum (src/suppress.rs:10-107) for the reference's integer
+ * channel types (Primitive + Ord; usize/isize map to the 64-bit forms): `out`
+ * (width x height, row-major) holds a pixel's value where it is the greatest
+ * in the (2 * radius + 1)^2 window centred on it (clipped to the image) and
+ * zero elsewhere; among equal values the lexicographically smaller (x, y)
+ * wins. The f32 form is additive (f32 is not Ord in the reference), for score
+ * maps: values compare in IEEE total order (-0 below +0, NaN above every
+ * number). The device
+ * forms are enqueued on `stream` and use the calling thread's scratch. */
+#define IPB_DECLARE_SUPPRESS(T, S)                                                        \
+    ipb_status ipb_suppress_non_maximum_##S(const T *image, uint32_t width, uint32_t height, \
+                                            uint32_t radius, T *out);                    \
+    ipb_status ipb_suppress_non_maximum_##S##_device(const T *d_image, uint32_t width,      \
+                                                     uint32_t height, uint32_t radius,     \
+                                                     T *d_out, void *stream);
+
+IPB_DECLARE_SUPPRESS(uint8_t, u8)
+IPB_DECLARE_SUPPRESS(uint16_t, u16)
+IPB_DECLARE_SUPPRESS(uint32_t, u32)
+IPB_DECLARE_SUPPRESS(uint64_t, u64)
+IPB_DECLARE_SUPPRESS(int8_t, i8)
+IPB_DECLARE_SUPPRESS(int16_t, i16)
+IPB_DECLARE_SUPPRESS(int32_t, i32)
+IPB_DECLARE_SUPPRESS(int64_t, i64)
+IPB_DECLARE_SUPPRESS(float, f32)
+
+/* local_maxima (src/suppress.rs:111-173) of n scored points (x, y, score):
+ * writes to out_indices the input indices of the points the reference
+ * returns, in its order (points sorted by (y, x), equal positions in input
+ * order), and their number to *out_count. out_indices holds n entries. */
+ipb_status ipb_local_maxima(const uint32_t *xs, const uint32_t *ys, const float *scores, uint32_t n,
+                            uint32_t radius, uint32_t *out_indices, uint32_t *out_count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,12 @@ def lib() -> C.CDLL:
         L.tmo_finish.restype = C.c_float
         L.tmo_find_extremes_index.argtypes = [C.c_void_p, u32, u32, C.c_int,
                                               C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.nxo_integral_u32.argtypes = [u8p, u32, u32, u32, C.c_int, C.c_void_p]
+        L.nxo_integral_u64.argtypes = [u8p, u32, u32, u32, C.c_int, C.c_void_p]
+        L.nxo_suppress_non_maximum.argtypes = [C.c_void_p, u32, u32, u32, C.c_void_p]
+        L.nxo_suppress_non_maximum_naive.argtypes = [C.c_void_p, u32, u32, u32, C.c_void_p]
+        L.nxo_local_maxima.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, u32, u32, C.c_void_p]
+        L.nxo_local_maxima.restype = u32
         _lib = L
     return _lib
 
@@ -129,3 +135,58 @@ def find_extremes(image):
     flat = a.reshape(-1)
     return (flat[imax.value], flat[imin.value], (imax.value % W, imax.value // W),
             (imin.value % W, imin.value // W))
+
+
+# ---- integral images and non-maximum suppression (next_oracle.c) ------------
+
+def order_keys(a) -> np.ndarray:
+    """u64 keys that compare like the values of `a` (any integer or float dtype)."""
+    a = np.ascontiguousarray(a)
+    if a.dtype.kind == "u":
+        return a.astype(np.uint64)
+    if a.dtype.kind == "i":
+        return a.astype(np.int64).view(np.uint64) ^ np.uint64(1 << 63)
+    if a.dtype == np.float32:
+        b = a.view(np.uint32).astype(np.uint64)
+        return np.where(b >> np.uint64(31), ~b & np.uint64(0xFFFFFFFF), b | np.uint64(0x80000000))
+    if a.dtype == np.float64:
+        b = a.view(np.uint64)
+        return np.where(b >> np.uint64(63), ~b, b | np.uint64(1 << 63))
+    raise TypeError(f"no order keys for {a.dtype}")
+
+
+def integral_image(image, square=False, bits=32) -> np.ndarray:
+    """integral_image / integral_squared_image (src/integral_image.rs:98-153) of a
+    (H, W) or (H, W, C) u8 image: (H+1, W+1[, C]) of u32 (wrapping) or u64."""
+    a = np.ascontiguousarray(image, dtype=np.uint8)
+    H, W = a.shape[:2]
+    C = 1 if a.ndim == 2 else a.shape[2]
+    dt = np.uint32 if bits == 32 else np.uint64
+    out = np.empty((H + 1, W + 1, C), dt)
+    f = lib().nxo_integral_u32 if bits == 32 else lib().nxo_integral_u64
+    f(_p(a), W, H, C, int(bool(square)), _p(out))
+    return out[:, :, 0] if a.ndim == 2 else out
+
+
+def suppress_non_maximum(image, radius, naive=False) -> np.ndarray:
+    """suppress_non_maximum (src/suppress.rs:10-107); naive=True follows the
+    reference tests' own definition (:274-318)."""
+    a = np.ascontiguousarray(image)
+    H, W = a.shape
+    keys = np.ascontiguousarray(order_keys(a))
+    keep = np.zeros((H, W), np.uint8)
+    f = lib().nxo_suppress_non_maximum_naive if naive else lib().nxo_suppress_non_maximum
+    if H and W:
+        f(_p(keys), W, H, int(radius), _p(keep))
+    return np.where(keep.astype(bool), a, np.zeros((), a.dtype)).astype(a.dtype)
+
+
+def local_maxima(xs, ys, scores, radius) -> list[int]:
+    """local_maxima (src/suppress.rs:111-173): input indices of the kept points in
+    the reference's output order."""
+    xs = np.ascontiguousarray(xs, np.uint32)
+    ys = np.ascontiguousarray(ys, np.uint32)
+    sc = np.ascontiguousarray(scores, np.float32)
+    out = np.empty(max(len(xs), 1), np.uint32)
+    n = lib().nxo_local_maxima(_p(xs), _p(ys), _p(sc), len(xs), int(radius), _p(out))
+    return [int(i) for i in out[:n]]

@@ -18,6 +18,7 @@ from imageproc_b200 import template_matching as tm
 
 HEADER = ROOT / "include" / "imageproc_b200.h"
 EXTREMES_SUFFIXES = ["u8", "u16", "u32", "u64", "i8", "i16", "i32", "i64", "f32", "f64"]
+SUPPRESS_SUFFIXES = ["u8", "u16", "u32", "u64", "i8", "i16", "i32", "i64", "f32"]
 
 
 def declared_functions():
@@ -29,6 +30,10 @@ def declared_functions():
     for s in EXTREMES_SUFFIXES:
         names.add(f"ipb_find_extremes_{s}")
         names.add(f"ipb_find_extremes_{s}_device")
+    # and so is suppress_non_maximum's
+    for s in SUPPRESS_SUFFIXES:
+        names.add(f"ipb_suppress_non_maximum_{s}")
+        names.add(f"ipb_suppress_non_maximum_{s}_device")
     names = {n for n in names if not n.startswith("ipb_extremes_")}
     return sorted(names)
 

@@ -1,0 +1,155 @@
+"""Integral images and non-maximum suppression on the GPU against the oracle
+(src/integral_image.rs, src/suppress.rs). Bar: bit-exact tables and outputs,
+identical point lists."""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from imageproc_b200 import integral_image as ii
+from imageproc_b200 import suppress as sp
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_next_tests.json").read_text())
+
+
+def case(section, name):
+    return next(c for c in GOLDEN[section]["cases"] if c["name"] == name)
+
+
+# ---- integral images ------------------------------------------------------------
+
+SHAPES = [(2, 3), (1, 1), (7, 1), (1, 9), (37, 53), (256, 300), (513, 1031), (1080, 1920)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("channels", [1, 3, 4])
+def test_integral_tables_bit_exact(shape, channels):
+    g = np.random.default_rng(shape[0] * 7 + channels)
+    img = g.integers(0, 256, shape if channels == 1 else shape + (channels,), dtype=np.uint8)
+    for square in (False, True):
+        for dtype, bits in ((np.uint32, 32), (np.uint64, 64)):
+            fn = ii.integral_squared_image if square else ii.integral_image
+            got = fn(img, dtype)
+            assert np.array_equal(got, O.integral_image(img, square=square, bits=bits)), (square, bits)
+
+
+def test_integral_golden_and_empty():
+    for name in ("test_integral_image_gray", "test_integral_squared_image_gray", "test_integral_image_rgb"):
+        c = case("integral_image", name)
+        img = np.array(c["image"]["rows"], np.uint8)
+        fn = ii.integral_squared_image if c["square"] else ii.integral_image
+        assert np.array_equal(fn(img), np.array(c["expected"]["rows"], np.uint32))
+    for W, H in ((0, 5), (4, 0), (0, 0)):
+        t = ii.integral_image(np.zeros((H, W), np.uint8))
+        assert t.shape == (H + 1, W + 1) and not t.any()
+
+
+def test_integral_u32_wraps_like_the_reference():
+    img = np.full((4100, 4100), 255, np.uint8)  # sum of squares > 2^32
+    got = ii.integral_squared_image(img, np.uint32)
+    exact = ii.integral_squared_image(img, np.uint64)
+    assert int(exact[-1, -1]) > 2**32
+    assert np.array_equal(got, (exact & 0xFFFFFFFF).astype(np.uint32))
+
+
+def test_integral_device_form():
+    import ctypes as C
+
+    import torch
+
+    from imageproc_b200 import _lib
+    g = np.random.default_rng(1)
+    img = g.integers(0, 256, (123, 77, 3), dtype=np.uint8)
+    d_img = torch.from_numpy(img).cuda()
+    d_out = torch.empty((124, 78, 3), dtype=torch.int64, device="cuda")
+    L = _lib.lib()
+    L.ipb_integral_image_device.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_void_p]
+    L.ipb_integral_image_device.restype = C.c_int
+    _lib.check(L.ipb_integral_image_device(d_img.data_ptr(), 77, 123, 3, 1, 64, d_out.data_ptr(),
+                                           torch.cuda.current_stream().cuda_stream or None))
+    torch.cuda.synchronize()
+    assert np.array_equal(d_out.cpu().numpy().view(np.uint64), O.integral_image(img, square=True, bits=64))
+
+
+# ---- suppress_non_maximum ---------------------------------------------------------
+
+DTYPES = [np.uint8, np.uint16, np.uint32, np.uint64, np.int8, np.int16, np.int32, np.int64, np.float32]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_suppress_matches_oracle_with_ties(dtype):
+    g = np.random.default_rng(np.dtype(dtype).num)
+    signed = np.dtype(dtype).kind in "if"
+    for _ in range(40):
+        H, W = int(g.integers(1, 40)), int(g.integers(1, 40))
+        a = g.integers(-4 if signed else 0, 5, (H, W)).astype(dtype)  # few values: many ties
+        r = int(g.integers(0, 9))
+        assert np.array_equal(sp.suppress_non_maximum(a, r), O.suppress_non_maximum(a, r)), (H, W, r)
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.int32, np.uint64, np.float32])
+def test_suppress_full_range_values(dtype):
+    g = np.random.default_rng(3)
+    info = np.finfo(dtype) if np.dtype(dtype).kind == "f" else np.iinfo(dtype)
+    if np.dtype(dtype).kind == "f":
+        a = g.standard_normal((300, 500)).astype(dtype) * 1e3
+        a[0, :5] = [0.0, -0.0, np.inf, -np.inf, np.nan]
+    else:
+        a = g.integers(info.min, info.max, (300, 500), dtype=dtype, endpoint=True)
+    for r in (1, 3, 16):
+        got = sp.suppress_non_maximum(a, r)
+        exp = O.suppress_non_maximum(a, r)
+        assert np.array_equal(got.view(np.uint8), exp.view(np.uint8)), r
+
+
+def test_suppress_golden_and_edges():
+    c = case("suppress", "test_suppress_non_maximum")
+    W, H = c["size"]
+    img = np.zeros((H, W), np.uint8)
+    for x, y, v in c["pixels"]:
+        img[y, x] = v
+    exp = np.zeros((H, W), np.uint8)
+    for x, y, v in c["expected"]:
+        exp[y, x] = v
+    assert np.array_equal(sp.suppress_non_maximum(img, c["radius"]), exp)
+    c = case("suppress", "test_suppress_non_maximum_handles_radius_greater_than_image_side")
+    for W, H in c["sizes"]:
+        a = np.random.default_rng(W).integers(0, 3, (H, W)).astype(np.uint8)
+        assert np.array_equal(sp.suppress_non_maximum(a, c["radius"]), O.suppress_non_maximum(a, c["radius"]))
+    assert sp.suppress_non_maximum(np.zeros((0, 5), np.uint8), 3).shape == (0, 5)
+
+
+def test_suppress_wide_radius_and_large_image():
+    g = np.random.default_rng(11)
+    a = g.integers(0, 6, (50, 40)).astype(np.uint16)
+    assert np.array_equal(sp.suppress_non_maximum(a, 3000), O.suppress_non_maximum(a, 3000))  # global-memory rows
+    b = g.integers(0, 50, (1080, 1920)).astype(np.uint8)
+    assert np.array_equal(sp.suppress_non_maximum(b, 5), O.suppress_non_maximum(b, 5))
+
+
+# ---- local_maxima -------------------------------------------------------------------
+
+def test_local_maxima_golden():
+    c = case("suppress", "test_local_maxima")
+    pts = [tuple(p) for p in c["points"]]
+    assert [list(p) for p in sp.local_maxima(pts, c["radius"])] == c["expected"]
+    assert sp.local_maxima([], 3) == []
+
+
+def test_local_maxima_matches_oracle():
+    g = np.random.default_rng(5)
+    for trial in range(60):
+        n = int(g.integers(1, 400))
+        span = int(g.integers(1, 60))
+        xs = g.integers(0, span, n).astype(np.uint32)
+        ys = g.integers(0, span, n).astype(np.uint32)
+        sc = g.integers(0, 6, n).astype(np.float32)  # ties and duplicate positions
+        if trial % 5 == 0:
+            sc[g.integers(0, n, 3)] = np.nan
+        r = int(g.integers(0, 8))
+        assert sp.local_maxima_indices(xs, ys, sc, r) == O.local_maxima(xs, ys, sc, r), trial
