@@ -41,6 +41,13 @@ device-resident and through the host API) and `batch_uneven` (256 uneven
 (image, template, method) pairs, image sides log-uniform in 256..4096,
 template sides 8..128, as one planned batch replayed as a CUDA graph with
 every map's find_extremes fused).
+
+`next_rows` measures the rows beside the matching path, each against the HBM
+roofline (algorithmic bytes: input read once, output written once) with the
+oracle's single-thread C restatement of the reference timed on the same
+input: integral_squared_image (u64) of a 4096x4096 scene,
+suppress_non_maximum (radius 8) of a 4065x4065 f32 score map, and
+local_maxima (radius 8) of 100k scored points.
 """
 
 from __future__ import annotations
@@ -364,6 +371,99 @@ def run_side_configs(args, world, rank, local) -> dict:
     return res
 
 
+def run_next_rows(args, world, rank, local) -> dict:
+    """Integral image, non-maximum suppression and local maxima."""
+    import ctypes as C
+
+    import torch
+
+    from imageproc_b200 import _lib, synthetic
+    from imageproc_b200 import suppress as sp
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    L = _lib.lib()
+    sh = stream.cuda_stream or None
+    pk = peaks()
+    res = {}
+
+    def roof(nbytes, ms):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": gbs / pk["hbm_gbs"], "traffic": None}
+
+    # integral_squared_image, u64, 4096 x 4096
+    side = 4096
+    img = synthetic.value_noise(side, side, 4 + rank)
+    d_img = torch.from_numpy(img).to(dev)
+    d_sat = torch.empty(((side + 1) * (side + 1),), dtype=torch.int64, device=dev)
+    L.ipb_integral_image_device.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_void_p]
+    L.ipb_integral_image_device.restype = C.c_int
+    sat = lambda: _lib.check(L.ipb_integral_image_device(d_img.data_ptr(), side, side, 1, 1, 64,  # noqa: E731
+                                                         d_sat.data_ptr(), sh))
+    for _ in range(3):
+        sat()
+    ms = max_over_ranks(_timed(sat, 10, flush, stream), world)
+    nbytes = side * side + (side + 1) ** 2 * 8
+    t0 = time.perf_counter()
+    O.integral_image(img, square=True, bits=64)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    res["integral_squared_image"] = {
+        "workload": f"value_noise {side}x{side} u8 -> ({side}+1)^2 u64 table", "ms": ms,
+        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9, "roofline": roof(nbytes, ms),
+        "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
+                         "sample": "the whole table, oracle restatement of src/integral_image.rs:98-153"}}
+    del d_sat
+
+    # suppress_non_maximum, radius 8, of a 4065 x 4065 f32 score map
+    wo = 4065
+    g = np.random.default_rng(rank)
+    smap = g.random((wo, wo), dtype=np.float32)
+    d_map = torch.from_numpy(smap).to(dev)
+    d_nms = torch.empty_like(d_map)
+    f = L.ipb_suppress_non_maximum_f32_device
+    f.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    nms = lambda: _lib.check(f(d_map.data_ptr(), wo, wo, 8, d_nms.data_ptr(), sh))  # noqa: E731
+    for _ in range(3):
+        nms()
+    ms = max_over_ranks(_timed(nms, 10, flush, stream), world)
+    band = smap[:512]
+    t0 = time.perf_counter()
+    O.suppress_non_maximum(band, 8)
+    cpu_ms = (time.perf_counter() - t0) * 1e3 * (wo / 512)
+    res["suppress_non_maximum"] = {
+        "workload": f"uniform f32 score map {wo}x{wo}, radius 8", "ms": ms,
+        "gpix_per_s": world * wo * wo / (ms / 1e3) / 1e9, "roofline": roof(2 * 4 * wo * wo, ms),
+        "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
+                         "sample": "512 of 4065 rows, oracle restatement of src/suppress.rs:10-107, scaled by rows"}}
+    del d_map, d_nms
+
+    # local_maxima, radius 8, of 100k scored points on a 4096 x 4096 grid
+    n = 100_000
+    xs = g.integers(0, side, n).astype(np.uint32)
+    ys = g.integers(0, side, n).astype(np.uint32)
+    sc = g.random(n, dtype=np.float32)
+    sp.local_maxima_indices(xs, ys, sc, 8)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        kept = sp.local_maxima_indices(xs, ys, sc, 8)
+    ms = max_over_ranks((time.perf_counter() - t0) / 5 * 1e3, world)
+    t0 = time.perf_counter()
+    O.local_maxima(xs, ys, sc, 8)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    res["local_maxima"] = {
+        "workload": f"{n} points uniform on {side}x{side}, f32 scores, radius 8 ({len(kept)} kept)",
+        "ms": ms, "mpoints_per_s": world * n / (ms / 1e3) / 1e6,
+        "api": "ipb_local_maxima (host arrays in and out, copies inside the time)",
+        "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
+                         "sample": "all points, oracle restatement of src/suppress.rs:111-173"}}
+    return res
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -444,6 +544,7 @@ def run_ours(args, world, rank, local):
     del batch, plan
     many = None if args.no_many else run_many(args, world, rank, local)
     side = {} if args.no_many else run_side_configs(args, world, rank, local)
+    nxt = None if args.no_many else run_next_rows(args, world, rank, local)
     if rank != 0:
         return
     pk = peaks()
@@ -497,6 +598,7 @@ def run_ours(args, world, rank, local):
         "clocks": clk.summary(),
         "many_templates": many,
         **side,
+        "next_rows": nxt,
     }
     print(json.dumps(line), flush=True)
 
@@ -512,6 +614,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-many", action="store_true", help="skip the many-templates workload")
     ap.add_argument("--only-many", action="store_true", help="run the many-templates workload alone")
+    ap.add_argument("--only-next", action="store_true",
+                    help="run the integral-image / suppression measurements alone")
     ap.add_argument("--many-side", type=int, default=4096)
     ap.add_argument("--many-templates", type=int, default=512)
     ap.add_argument("--many-steps", type=int, default=5)
@@ -521,6 +625,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.only_next:
+            nxt = run_next_rows(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(nxt), flush=True)
         elif args.only_many:
             many = run_many(args, world, rank, local)
             if rank == 0:

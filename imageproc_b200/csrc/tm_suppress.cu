@@ -131,6 +131,52 @@ __global__ void __launch_bounds__(256) snm_cols_kernel(const T* __restrict__ img
   out[(size_t)y * W + x] = (wx == x && wy == y) ? v : T(0);
 }
 
+// Column pass through a shared-memory tile of 32 columns x 32 output rows and
+// r halo rows above and below: every row winner of the tile is gathered once
+// (its column and key, loads independent across the block), then each thread
+// scans its column window in shared memory.
+constexpr int kColTile = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict__ img, uint32_t W, uint32_t H,
+                                                            uint32_t r, const uint32_t* __restrict__ bx,
+                                                            T* __restrict__ out) {
+  extern __shared__ unsigned long long s_wk[];  // [kColTile + 2r][32] winner keys, then [..][32] columns
+  const uint32_t trows = kColTile + 2 * r;
+  uint32_t* s_wx = reinterpret_cast<uint32_t*>(s_wk + (size_t)trows * 32);
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t x = blockIdx.x * 32 + lane;
+  const uint32_t y0 = blockIdx.y * kColTile;
+  const uint32_t lo = y0 > r ? y0 - r : 0u;
+  const uint32_t hi = (uint32_t)min((unsigned long long)H, (unsigned long long)y0 + kColTile + r);
+  if (x < W)
+    for (uint32_t i = warp; i < hi - lo; i += 8) {
+      const uint32_t yy = lo + i, cx = bx[(size_t)yy * W + x];
+      s_wx[i * 32 + lane] = cx;
+      s_wk[i * 32 + lane] = okey(img[(size_t)yy * W + cx]);
+    }
+  __syncthreads();
+  if (x >= W) return;
+  for (uint32_t k = 0; k < kColTile / 8; ++k) {
+    const uint32_t y = y0 + warp * (kColTile / 8) + k;
+    if (y >= H) break;
+    const uint32_t a = y > r ? y - r : 0u;
+    const uint32_t b = (uint32_t)min((unsigned long long)H - 1, (unsigned long long)y + r);
+    uint32_t wx = s_wx[(a - lo) * 32 + lane], wy = a;
+    unsigned long long wk = s_wk[(a - lo) * 32 + lane];
+    for (uint32_t yy = a + 1; yy <= b; ++yy) {
+      const uint32_t cx = s_wx[(yy - lo) * 32 + lane];
+      const unsigned long long kk = s_wk[(yy - lo) * 32 + lane];
+      if (kk > wk || (kk == wk && cx < wx)) {
+        wk = kk;
+        wx = cx;
+        wy = yy;
+      }
+    }
+    out[(size_t)y * W + x] = (wx == x && wy == y) ? img[(size_t)y * W + x] : T(0);
+  }
+}
+
 template <typename T>
 cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, uint32_t* bx, cudaStream_t s) {
   if (W == 0 || H == 0) return cudaSuccess;
@@ -143,8 +189,15 @@ cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* ou
   count_launch(kKernelSuppress);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if ((H + 7) / 8 > 65535u) return cudaErrorInvalidValue;  // images up to 524280 rows
-  snm_cols_kernel<T><<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, s>>>(img, W, H, r, bx, out);
+  const size_t tile_bytes = ((size_t)kColTile + 2 * (size_t)r) * 32 * 12;
+  if (tile_bytes <= 48 * 1024) {
+    if ((H + kColTile - 1) / kColTile > 65535u) return cudaErrorInvalidValue;  // images up to 2097120 rows
+    snm_cols_tile_kernel<T><<<dim3((W + 31) / 32, (H + kColTile - 1) / kColTile), 256, tile_bytes, s>>>(
+        img, W, H, r, bx, out);
+  } else {
+    if ((H + 7) / 8 > 65535u) return cudaErrorInvalidValue;  // images up to 524280 rows
+    snm_cols_kernel<T><<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, s>>>(img, W, H, r, bx, out);
+  }
   count_launch(kKernelSuppress);
   return cudaGetLastError();
 }
