@@ -168,6 +168,101 @@ __device__ __forceinline__ uint32_t order_key(float f) {
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// A builder warp's share of a tile's epilogue: columns [c_begin, c_begin +
+// ncols) of the accumulators for its 32 lanes (output columns).
+struct UmmaEpi {
+  const UmmaProblem* q;
+  uint32_t tmem, lane_base, c_begin, ncols, NT, nrows, m, x, y0, tss, lane;
+  const uint32_t* s_rs;  // unmasked: row sums of squares of the tile's image rows
+  uint32_t Y;            // unmasked: window sum of the first column (row c_begin)
+};
+
+// Scores with the method and precision fixed at compile time, so the 16
+// scores of each tensor-memory load are straight-line code.
+template <bool MASKED, int kMethod, int kPrec, bool kExt>
+__device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
+  const UmmaProblem& q = *e.q;
+  uint32_t Y = e.Y;
+  unsigned long long kmin = ~0ull, kmax = 0ull;
+  for (uint32_t n0 = e.c_begin; n0 < e.c_begin + e.ncols; n0 += 16) {
+    uint32_t vx[16];
+    tmem_ld16(tmem_addr(e.tmem, e.lane_base, n0), vx);
+    uint32_t vl[MASKED ? 16 : 1], vh[MASKED ? 16 : 1];
+    uint32_t yv[16];
+    if constexpr (MASKED) {
+      tmem_ld16(tmem_addr(e.tmem, e.lane_base, e.NT + n0), vl);
+      tmem_ld16(tmem_addr(e.tmem, e.lane_base, 2 * e.NT + n0), vh);
+    } else {
+      // window sums of the chunk: loads first, then the sliding chain
+      uint32_t add[16], subv[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t ra = n0 + k + q.h, rb = n0 + k;
+        add[k] = ra < e.nrows ? e.s_rs[ra * kM + e.m] : 0u;
+        subv[k] = rb < e.nrows ? e.s_rs[rb * kM + e.m] : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        yv[k] = Y;
+        Y += add[k];
+        Y -= subv[k];
+      }
+    }
+    tmem_wait_ld();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t y = e.y0 + n0 + k;
+      uint32_t Yk;
+      if constexpr (MASKED) Yk = vl[k] + (vh[k] << 8);
+      else Yk = yv[k];
+      if (e.x < q.Wo && y < q.Ho) {
+        const float f = finish_score32(kMethod, kPrec, vx[k], Yk, e.tss);
+        const uint32_t lin = y * q.Wo + e.x;
+        q.out[(size_t)lin] = f;
+        if constexpr (kExt) {
+          const unsigned long long key = (unsigned long long)order_key(f) << 32;
+          kmin = min(kmin, key | lin);
+          kmax = max(kmax, key | (0xFFFFFFFFu - lin));
+        }
+      }
+    }
+  }
+  if constexpr (kExt) {
+    // first occurrence wins: min key = (smallest value, smallest index);
+    // max key = (largest value, smallest index) via the complemented index
+    for (int o = 16; o > 0; o >>= 1) {
+      kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+      kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    }
+    if (e.lane == 0 && kmin != ~0ull) {
+      atomicMin(q.ext, kmin);
+      atomicMax(q.ext + 1, kmax);
+    }
+  }
+}
+
+template <bool MASKED, int kMethod>
+__device__ __forceinline__ void umma_epilogue_m(const UmmaEpi& e, bool fp64, bool ext) {
+  if constexpr (!method_is_norm(kMethod)) fp64 = true;  // precision only affects the normalisation
+  if (fp64) {
+    if (ext) umma_epilogue<MASKED, kMethod, IPB_PRECISION_EXACT_FP64, true>(e);
+    else umma_epilogue<MASKED, kMethod, IPB_PRECISION_EXACT_FP64, false>(e);
+  } else {
+    if (ext) umma_epilogue<MASKED, kMethod, IPB_PRECISION_EXACT_F32, true>(e);
+    else umma_epilogue<MASKED, kMethod, IPB_PRECISION_EXACT_F32, false>(e);
+  }
+}
+
+template <bool MASKED>
+__device__ __forceinline__ void umma_epilogue_dispatch(const UmmaEpi& e, int method, bool fp64, bool ext) {
+  switch (method) {
+    case kSse: umma_epilogue_m<MASKED, kSse>(e, fp64, ext); break;
+    case kSseNorm: umma_epilogue_m<MASKED, kSseNorm>(e, fp64, ext); break;
+    case kCcorr: umma_epilogue_m<MASKED, kCcorr>(e, fp64, ext); break;
+    default: umma_epilogue_m<MASKED, kCcorrNorm>(e, fp64, ext); break;
+  }
+}
+
 template <int KS, bool MASKED>
 __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_constant__ UmmaLaunch L) {
   constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, low, high byte of I^2)
@@ -219,7 +314,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
 
   uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
   uint32_t tcount = 0;       // tiles finished by this CTA
-  uint32_t zp_loaded = ~0u;  // problem whose Z buffers and TSS are in shared memory
+  // template side whose Z buffers and TSS are in shared memory (consecutive
+  // problems of a batch often share it: several methods of one pair, one
+  // template over several images)
+  const uint8_t* z_tpl = nullptr;
+  const uint8_t* z_mask = nullptr;
+  uint32_t z_w = 0, z_h = 0, z_kmma = 0;
   uint32_t tss = 0;
   bool ok = true;
 
@@ -238,7 +338,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     const uint32_t y0 = (lt / q.tiles_x) * L.NT;
     const uint32_t nrows = min(q.rows_max, q.H - y0);
     const uint32_t zplane = (q.kmma / 16) * q.zrows * 16;
-    if (pi != zp_loaded) {
+    const bool new_z = q.tpl != z_tpl || q.mask != z_mask || q.w != z_w || q.h != z_h || q.kmma != z_kmma;
+    if (new_z) {
       // Z buffers, K-chunk-major: chunk c holds rows j = 0..zrows-1 of 16 bytes,
       // row j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
       //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m
@@ -282,11 +383,15 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     cp_async_wait_all();
     __syncthreads();
     if (*s_err) break;
-    if (pi != zp_loaded) {
+    if (new_z) {
       unsigned long long t = 0;
       for (int k = 0; k < kWarps; ++k) t += s_part[k];
       tss = (uint32_t)t;  // < 2^31: at most 33025 template pixels
-      zp_loaded = pi;
+      z_tpl = q.tpl;
+      z_mask = q.mask;
+      z_w = q.w;
+      z_h = q.h;
+      z_kmma = q.kmma;
     }
     if constexpr (MASKED) {
       // byte planes of I^2 next to the staged image
@@ -374,62 +479,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
           for (; r < c_begin + q.h; ++r) y4[0] += r < nrows ? s_rs[r * kM + m] : 0u;
           Y = y4[0] + y4[1] + y4[2] + y4[3];
         }
-        unsigned long long kmin = ~0ull, kmax = 0ull;
-        for (uint32_t n0 = c_begin; n0 < c_begin + ncols; n0 += 16) {
-          uint32_t vx[16];
-          tmem_ld16(tmem_addr(tmem, lane_base, n0), vx);
-          uint32_t vl[MASKED ? 16 : 1], vh[MASKED ? 16 : 1];
-          uint32_t yv[16];
-          if constexpr (MASKED) {
-            tmem_ld16(tmem_addr(tmem, lane_base, L.NT + n0), vl);
-            tmem_ld16(tmem_addr(tmem, lane_base, 2 * L.NT + n0), vh);
-          } else {
-            // window sums of the chunk: loads first, then the sliding chain
-            uint32_t add[16], subv[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              const uint32_t ra = n0 + k + q.h, rb = n0 + k;
-              add[k] = ra < nrows ? s_rs[ra * kM + m] : 0u;
-              subv[k] = rb < nrows ? s_rs[rb * kM + m] : 0u;
-            }
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-              yv[k] = Y;
-              Y += add[k];
-              Y -= subv[k];
-            }
-          }
-          tmem_wait_ld();
-#pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const uint32_t y = y0 + n0 + k;
-            uint32_t Yk;
-            if constexpr (MASKED) Yk = vl[k] + (vh[k] << 8);
-            else Yk = yv[k];
-            if (x < q.Wo && y < q.Ho) {
-              const float f = finish_score32(q.method, q.precision, vx[k], Yk, tss);
-              const uint32_t lin = y * q.Wo + x;
-              q.out[(size_t)lin] = f;
-              if (q.ext) {
-                const unsigned long long key = (unsigned long long)order_key(f) << 32;
-                kmin = min(kmin, key | lin);
-                kmax = max(kmax, key | (0xFFFFFFFFu - lin));
-              }
-            }
-          }
-        }
-        if (q.ext) {
-          // first occurrence wins: min key = (smallest value, smallest index);
-          // max key = (largest value, smallest index) via the complemented index
-          for (int o = 16; o > 0; o >>= 1) {
-            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-          }
-          if (lane == 0 && kmin != ~0ull) {
-            atomicMin(q.ext, kmin);
-            atomicMax(q.ext + 1, kmax);
-          }
-        }
+        const UmmaEpi e{&q, tmem, lane_base, c_begin, ncols, L.NT, nrows, m, x, y0, tss, (uint32_t)lane, s_rs, Y};
+        umma_epilogue_dispatch<MASKED>(e, q.method, q.precision == IPB_PRECISION_EXACT_FP64, q.ext != nullptr);
       }
       if (!ok) {
         *s_err = 1;
