@@ -46,7 +46,8 @@ every map's find_extremes fused).
 roofline (algorithmic bytes: input read once, output written once) with the
 oracle's single-thread C restatement of the reference timed on the same
 input: integral_squared_image (u64) of a 4096x4096 scene,
-suppress_non_maximum (radius 8) of a 4065x4065 f32 score map, and
+suppress_non_maximum (radius 8) of a 4065x4065 f32 score map,
+filter_clamped (5x5 f32 kernel) of the 4096x4096 scene into u8, and
 local_maxima (radius 8) of 100k scored points.
 """
 
@@ -372,7 +373,7 @@ def run_side_configs(args, world, rank, local) -> dict:
 
 
 def run_next_rows(args, world, rank, local) -> dict:
-    """Integral image, non-maximum suppression and local maxima."""
+    """Integral image, non-maximum suppression, filter_clamped and local maxima."""
     import ctypes as C
 
     import torch
@@ -441,6 +442,29 @@ def run_next_rows(args, world, rank, local) -> dict:
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "512 of 4065 rows, oracle restatement of src/suppress.rs:10-107, scaled by rows"}}
     del d_map, d_nms
+
+    # filter_clamped, 5 x 5 f32 kernel, 4096 x 4096 u8 -> u8
+    kern = (g.random((5, 5), dtype=np.float32) / np.float32(12.5)).astype(np.float32)
+    d_k = torch.from_numpy(kern).to(dev)
+    d_f = torch.empty_like(d_img)
+    ff = L.ipb_filter_clamped_device
+    ff.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_int, C.c_uint32, C.c_uint32,
+                   C.c_int, C.c_void_p, C.c_void_p]
+    ff.restype = C.c_int
+    flt = lambda: _lib.check(ff(d_img.data_ptr(), side, side, 1, d_k.data_ptr(), 0, 5, 5, 0,  # noqa: E731
+                                d_f.data_ptr(), sh))
+    for _ in range(3):
+        flt()
+    ms = max_over_ranks(_timed(flt, 10, flush, stream), world)
+    t0 = time.perf_counter()
+    O.filter_clamped(img[:512], kern, np.uint8)
+    cpu_ms = (time.perf_counter() - t0) * 1e3 * (side / 512)
+    res["filter_clamped"] = {
+        "workload": f"value_noise {side}x{side} u8, 5x5 f32 kernel, clamped to u8", "ms": ms,
+        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9, "roofline": roof(2 * side * side, ms),
+        "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
+                         "sample": "512 of 4096 rows, oracle restatement of src/filter/mod.rs:29-70, scaled by rows"}}
+    del d_f, d_k
 
     # local_maxima, radius 8, of 100k scored points on a 4096 x 4096 grid
     n = 100_000

@@ -91,7 +91,7 @@ void note_timed(KernelTimer* t, double macs, double bytes) {
 const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
-      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress"};
+      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress", "filter"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -655,15 +655,15 @@ ipb_status device_suppress(int type, const void* d_image, uint32_t W, uint32_t H
                                                            uint32_t radius, T* d_out, void* stream) {   \
     return device_suppress(CODE, d_image, W, H, radius, d_out, stream);                                  \
   }
-IPB_DEFINE_SUPPRESS(uint8_t, u8, IPB_TYPE_U8)
-IPB_DEFINE_SUPPRESS(uint16_t, u16, IPB_TYPE_U16)
-IPB_DEFINE_SUPPRESS(uint32_t, u32, IPB_TYPE_U32)
-IPB_DEFINE_SUPPRESS(uint64_t, u64, IPB_TYPE_U64)
-IPB_DEFINE_SUPPRESS(int8_t, i8, IPB_TYPE_I8)
-IPB_DEFINE_SUPPRESS(int16_t, i16, IPB_TYPE_I16)
-IPB_DEFINE_SUPPRESS(int32_t, i32, IPB_TYPE_I32)
-IPB_DEFINE_SUPPRESS(int64_t, i64, IPB_TYPE_I64)
-IPB_DEFINE_SUPPRESS(float, f32, IPB_TYPE_F32)
+IPB_DEFINE_SUPPRESS(uint8_t, u8, IPB_ELEM_U8)
+IPB_DEFINE_SUPPRESS(uint16_t, u16, IPB_ELEM_U16)
+IPB_DEFINE_SUPPRESS(uint32_t, u32, IPB_ELEM_U32)
+IPB_DEFINE_SUPPRESS(uint64_t, u64, IPB_ELEM_U64)
+IPB_DEFINE_SUPPRESS(int8_t, i8, IPB_ELEM_I8)
+IPB_DEFINE_SUPPRESS(int16_t, i16, IPB_ELEM_I16)
+IPB_DEFINE_SUPPRESS(int32_t, i32, IPB_ELEM_I32)
+IPB_DEFINE_SUPPRESS(int64_t, i64, IPB_ELEM_I64)
+IPB_DEFINE_SUPPRESS(float, f32, IPB_ELEM_F32)
 #undef IPB_DEFINE_SUPPRESS
 
 IPB_API ipb_status ipb_local_maxima(const uint32_t* xs, const uint32_t* ys, const float* scores, uint32_t n,
@@ -695,6 +695,62 @@ IPB_API ipb_status ipb_local_maxima(const uint32_t* xs, const uint32_t* ys, cons
   IPB_CUDA(cudaMemcpyAsync(out_count, d_count, 4, cudaMemcpyDeviceToHost, c->stream), "copy count");
   IPB_CUDA(cudaMemcpyAsync(out_indices, d_out, nb, cudaMemcpyDeviceToHost, c->stream), "copy indices");
   return finish_sync(c, c->stream);
+}
+
+// ---- filter_clamped -------------------------------------------------------------------
+namespace {
+size_t elem_size(int type) {
+  switch (type) {
+    case IPB_ELEM_U8: case IPB_ELEM_I8: return 1;
+    case IPB_ELEM_U16: case IPB_ELEM_I16: return 2;
+    case IPB_ELEM_U32: case IPB_ELEM_I32: case IPB_ELEM_F32: return 4;
+    default: return 8;
+  }
+}
+
+ipb_status check_filter_args(uint32_t channels, int ktype, uint32_t kw, uint32_t kh, int otype) {
+  if (kw == 0 || kh == 0) return fail(IPB_ERR_INVALID_ARGUMENT, "width and height must be non-zero");
+  if (channels != 1 && channels != 3 && channels != 4)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "channels must be 1 (Luma), 3 (Rgb) or 4 (Rgba)");
+  if (!filter_types_supported(ktype, otype))
+    return fail(IPB_ERR_INVALID_ARGUMENT,
+                "no Clamp from this kernel type to this output type (f32 kernels: u8, u16, f32; i32 kernels: u8, "
+                "u16, i16, i32)");
+  return IPB_OK;
+}
+}  // namespace
+
+IPB_API ipb_status ipb_filter_clamped(const uint8_t* image, uint32_t W, uint32_t H, uint32_t channels,
+                                      const void* kernel, int kernel_type, uint32_t kw, uint32_t kh, int out_type,
+                                      void* out) {
+  ipb_status st = check_filter_args(channels, kernel_type, kw, kh, out_type);
+  if (st) return st;
+  const size_t ib = (size_t)W * H * channels, kb = (size_t)kw * kh * 4, ob = ib * elem_size(out_type);
+  if (!kernel || ((!image || !out) && ib)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!ib) return IPB_OK;
+  Context* c = nullptr;
+  if ((st = get_ctx(&c))) return st;
+  if ((st = ensure(c, c->img, ib)) || (st = ensure(c, c->tpl, kb)) || (st = ensure(c, c->out, ob))) return st;
+  IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(cudaMemcpyAsync(c->img.p, image, ib, cudaMemcpyHostToDevice, c->stream), "copy image");
+  IPB_CUDA(cudaMemcpyAsync(c->tpl.p, kernel, kb, cudaMemcpyHostToDevice, c->stream), "copy kernel");
+  IPB_CUDA(launch_filter(static_cast<const uint8_t*>(c->img.p), W, H, channels, c->tpl.p, kernel_type, kw, kh,
+                         out_type, c->out.p, c->stream),
+           "filter launch");
+  IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy output");
+  return finish_sync(c, c->stream);
+}
+
+IPB_API ipb_status ipb_filter_clamped_device(const uint8_t* d_image, uint32_t W, uint32_t H, uint32_t channels,
+                                             const void* d_kernel, int kernel_type, uint32_t kw, uint32_t kh,
+                                             int out_type, void* d_out, void* stream) {
+  ipb_status st = check_filter_args(channels, kernel_type, kw, kh, out_type);
+  if (st) return st;
+  if (!d_kernel || ((!d_image || !d_out) && (size_t)W * H)) return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  IPB_CUDA(launch_filter(d_image, W, H, channels, d_kernel, kernel_type, kw, kh, out_type, d_out,
+                         static_cast<cudaStream_t>(stream)),
+           "filter launch");
+  return IPB_OK;
 }
 
 IPB_API ipb_status ipb_match_template_device(const uint8_t* d_image, uint32_t W, uint32_t H,

@@ -22,6 +22,7 @@ enum KernelId : int {
   kKernelUmma,
   kKernelMany,
   kKernelSuppress,
+  kKernelFilter,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -92,11 +93,7 @@ cudaError_t launch_sat(const uint8_t* img, uint32_t W, uint32_t H, uint32_t chan
                        void* sat, cudaStream_t s);
 
 // ---- non-maximum suppression (tm_suppress.cu) -------------------------------
-enum ElemType : int {
-  IPB_TYPE_U8 = 0, IPB_TYPE_U16, IPB_TYPE_U32, IPB_TYPE_U64,
-  IPB_TYPE_I8, IPB_TYPE_I16, IPB_TYPE_I32, IPB_TYPE_I64, IPB_TYPE_F32
-};
-// suppress_non_maximum of a W x H image of `type`; bx = W*H u32 scratch.
+// suppress_non_maximum of a W x H image of element `type` (ipb_elem_type); bx = W*H u32 scratch.
 cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
                             cudaStream_t s);
 size_t local_maxima_scratch_bytes(uint32_t n, uint32_t max_y);
@@ -106,6 +103,14 @@ size_t local_maxima_scratch_bytes(uint32_t n, uint32_t max_y);
 cudaError_t launch_local_maxima(const uint32_t* xs, const uint32_t* ys, const float* scores, uint32_t n,
                                 uint32_t radius, uint32_t max_y, void* scratch, size_t scratch_bytes,
                                 uint32_t* out, uint32_t* count, cudaStream_t s);
+
+// ---- filter_clamped (tm_filter.cu) --------------------------------------------
+// whether the reference has a Clamp from the kernel type to the output type
+bool filter_types_supported(int ktype, int otype);
+// filter_clamped of a W x H u8 image with `channels` interleaved channels by a
+// kw x kh row-major kernel (device memory); out is W x H x channels of otype.
+cudaError_t launch_filter(const uint8_t* img, uint32_t W, uint32_t H, uint32_t channels, const void* kern, int ktype,
+                          uint32_t kw, uint32_t kh, int otype, void* out, cudaStream_t s);
 
 // ---- CUDA-core exact kernel (tm_exact_cc.cu) ------------------------------
 size_t exact_cc_scratch_bytes(const MatchArgs& a);

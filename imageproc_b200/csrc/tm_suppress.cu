@@ -269,22 +269,22 @@ __global__ void lm_compact_kernel(const uint32_t* flags, const uint32_t* pos, co
 cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
                             cudaStream_t s) {
   switch (type) {
-    case IPB_TYPE_U8: return launch_snm_t(static_cast<const uint8_t*>(img), W, H, r, static_cast<uint8_t*>(out), bx, s);
-    case IPB_TYPE_U16:
+    case IPB_ELEM_U8: return launch_snm_t(static_cast<const uint8_t*>(img), W, H, r, static_cast<uint8_t*>(out), bx, s);
+    case IPB_ELEM_U16:
       return launch_snm_t(static_cast<const uint16_t*>(img), W, H, r, static_cast<uint16_t*>(out), bx, s);
-    case IPB_TYPE_U32:
+    case IPB_ELEM_U32:
       return launch_snm_t(static_cast<const uint32_t*>(img), W, H, r, static_cast<uint32_t*>(out), bx, s);
-    case IPB_TYPE_U64:
+    case IPB_ELEM_U64:
       return launch_snm_t(static_cast<const unsigned long long*>(img), W, H, r,
                           static_cast<unsigned long long*>(out), bx, s);
-    case IPB_TYPE_I8: return launch_snm_t(static_cast<const int8_t*>(img), W, H, r, static_cast<int8_t*>(out), bx, s);
-    case IPB_TYPE_I16:
+    case IPB_ELEM_I8: return launch_snm_t(static_cast<const int8_t*>(img), W, H, r, static_cast<int8_t*>(out), bx, s);
+    case IPB_ELEM_I16:
       return launch_snm_t(static_cast<const int16_t*>(img), W, H, r, static_cast<int16_t*>(out), bx, s);
-    case IPB_TYPE_I32:
+    case IPB_ELEM_I32:
       return launch_snm_t(static_cast<const int32_t*>(img), W, H, r, static_cast<int32_t*>(out), bx, s);
-    case IPB_TYPE_I64:
+    case IPB_ELEM_I64:
       return launch_snm_t(static_cast<const long long*>(img), W, H, r, static_cast<long long*>(out), bx, s);
-    case IPB_TYPE_F32: return launch_snm_t(static_cast<const float*>(img), W, H, r, static_cast<float*>(out), bx, s);
+    case IPB_ELEM_F32: return launch_snm_t(static_cast<const float*>(img), W, H, r, static_cast<float*>(out), bx, s);
     default: return cudaErrorInvalidValue;
   }
 }

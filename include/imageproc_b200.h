@@ -77,6 +77,26 @@ typedef enum ipb_precision {
     IPB_PRECISION_REFERENCE_F32 = 2
 } ipb_precision;
 
+/* Element types of arrays passed to the non-matching entry points
+ * (suppression, filters): additive, no reference counterpart. */
+typedef enum ipb_elem_type {
+    IPB_ELEM_U8 = 0,
+    IPB_ELEM_U16 = 1,
+    IPB_ELEM_U32 = 2,
+    IPB_ELEM_U64 = 3,
+    IPB_ELEM_I8 = 4,
+    IPB_ELEM_I16 = 5,
+    IPB_ELEM_I32 = 6,
+    IPB_ELEM_I64 = 7,
+    IPB_ELEM_F32 = 8
+} ipb_elem_type;
+
+/* Accumulator (kernel element) type of filter_clamped. */
+typedef enum ipb_kernel_type {
+    IPB_KERNEL_TYPE_F32 = 0,
+    IPB_KERNEL_TYPE_I32 = 1
+} ipb_kernel_type;
+
 /* Message of the last failure on the calling thread ("" if none). */
 const char *ipb_last_error_message(void);
 
@@ -366,6 +386,28 @@ IPB_DECLARE_SUPPRESS(float, f32)
  * order), and their number to *out_count. out_indices holds n entries. */
 ipb_status ipb_local_maxima(const uint32_t *xs, const uint32_t *ys, const float *scores, uint32_t n,
                             uint32_t radius, uint32_t *out_indices, uint32_t *out_count);
+
+/* ---- filters ---------------------------------------------------------------------
+ * filter_clamped (src/filter/mod.rs:202-212, through filter :29-70): the 2-D
+ * correlation of a u8 image with `channels` interleaved channels (1, 3, 4) by a
+ * kernel_width x kernel_height row-major kernel of kernel_type (f32 or i32),
+ * padded by continuity, accumulated per channel in the kernel's type in the
+ * reference's order (rows of the kernel outer, columns inner; f32 rounds each
+ * multiply and add; i32 wraps like a release build) and clamped to out_type by
+ * the reference's Clamp (src/definitions.rs:114-190): f32 kernels to u8, u16
+ * or f32, i32 kernels to u8, u16, i16 or i32. Output: width x height x
+ * channels of out_type. A kernel with a zero side fails with the reference's
+ * message "width and height must be non-zero" (src/kernel.rs:25). With 1 x n
+ * and n x 1 kernels this is horizontal_filter / vertical_filter
+ * (src/filter/mod.rs:232, :319). */
+ipb_status ipb_filter_clamped(const uint8_t *image, uint32_t width, uint32_t height, uint32_t channels,
+                              const void *kernel, int kernel_type, uint32_t kernel_width,
+                              uint32_t kernel_height, int out_type, void *out);
+/* The same on device buffers (the kernel too), enqueued on `stream`. */
+ipb_status ipb_filter_clamped_device(const uint8_t *d_image, uint32_t width, uint32_t height,
+                                     uint32_t channels, const void *d_kernel, int kernel_type,
+                                     uint32_t kernel_width, uint32_t kernel_height, int out_type,
+                                     void *d_out, void *stream);
 
 #ifdef __cplusplus
 }

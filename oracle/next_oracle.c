@@ -164,3 +164,56 @@ uint32_t nxo_local_maxima(const uint32_t *xs, const uint32_t *ys, const float *s
     free(ord);
     return count;
 }
+
+/* ---- filter_clamped: src/filter/mod.rs:29-70, :407-416 -------------------- */
+
+/* Clamp<K> for S (src/definitions.rs:119-131): `if x < max { if x > min { x as S }
+ * else { min } } else { max }` -- NaN fails both tests and gives max. */
+static double clamp_d(double x, double lo, double hi) {
+    if (x < hi) return x > lo ? x : lo;
+    return hi;
+}
+
+void nxo_filter_clamped(const uint8_t *img, uint32_t W, uint32_t H, uint32_t C, const void *kernel,
+                        int kernel_type, uint32_t kw, uint32_t kh, int out_type, void *out) {
+    const int64_t kwi = kw, khi = kh, Wi = W, Hi = H;
+    for (int64_t y = 0; y < Hi; ++y)
+        for (int64_t x = 0; x < Wi; ++x) {
+            float accf[4] = {0, 0, 0, 0};
+            uint32_t acci[4] = {0, 0, 0, 0}; /* i32 arithmetic, wrapping */
+            for (int64_t ky = 0; ky < khi; ++ky) {
+                int64_t yp = y + ky - khi / 2;
+                yp = yp < 0 ? 0 : (yp > Hi - 1 ? Hi - 1 : yp);
+                for (int64_t kx = 0; kx < kwi; ++kx) {
+                    int64_t xp = x + kx - kwi / 2;
+                    xp = xp < 0 ? 0 : (xp > Wi - 1 ? Wi - 1 : xp);
+                    const uint8_t *p = img + ((size_t)yp * W + (size_t)xp) * C;
+                    for (uint32_t c = 0; c < C; ++c) {
+                        if (kernel_type == 0) {
+                            const float w = ((const float *)kernel)[ky * kwi + kx];
+                            const float prod = (float)p[c] * w;
+                            accf[c] = accf[c] + prod;
+                        } else {
+                            const int32_t w = ((const int32_t *)kernel)[ky * kwi + kx];
+                            acci[c] = acci[c] + (uint32_t)p[c] * (uint32_t)w;
+                        }
+                    }
+                }
+            }
+            for (uint32_t c = 0; c < C; ++c) {
+                const size_t o = ((size_t)y * W + (size_t)x) * C + c;
+                if (kernel_type == 0) {
+                    const float a = accf[c];
+                    if (out_type == 8) ((float *)out)[o] = a;
+                    else if (out_type == 0) ((uint8_t *)out)[o] = (uint8_t)clamp_d(a, 0.0, 255.0);
+                    else ((uint16_t *)out)[o] = (uint16_t)clamp_d(a, 0.0, 65535.0);
+                } else {
+                    const int32_t a = (int32_t)acci[c];
+                    if (out_type == 6) ((int32_t *)out)[o] = a;
+                    else if (out_type == 0) ((uint8_t *)out)[o] = (uint8_t)clamp_d(a, 0.0, 255.0);
+                    else if (out_type == 1) ((uint16_t *)out)[o] = (uint16_t)clamp_d(a, 0.0, 65535.0);
+                    else ((int16_t *)out)[o] = (int16_t)clamp_d(a, -32768.0, 32767.0);
+                }
+            }
+        }
+}

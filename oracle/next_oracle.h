@@ -43,6 +43,13 @@ void nxo_suppress_non_maximum_naive(const uint64_t *keys, uint32_t W, uint32_t H
 uint32_t nxo_local_maxima(const uint32_t *xs, const uint32_t *ys, const float *scores, uint32_t n,
                           uint32_t radius, uint32_t *out_idx);
 
+/* filter_clamped (src/filter/mod.rs:202-212 through filter :29-70,
+ * accumulate :407-416, Clamp src/definitions.rs:119-190): kernel_type 0 = f32,
+ * 1 = i32; out_type uses the library's element codes (0 u8, 1 u16, 5 i16,
+ * 6 i32, 8 f32). */
+void nxo_filter_clamped(const uint8_t *img, uint32_t W, uint32_t H, uint32_t C, const void *kernel,
+                        int kernel_type, uint32_t kw, uint32_t kh, int out_type, void *out);
+
 #ifdef __cplusplus
 }
 #endif

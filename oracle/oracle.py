@@ -51,6 +51,7 @@ def lib() -> C.CDLL:
         L.nxo_suppress_non_maximum_naive.argtypes = [C.c_void_p, u32, u32, u32, C.c_void_p]
         L.nxo_local_maxima.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, u32, u32, C.c_void_p]
         L.nxo_local_maxima.restype = u32
+        L.nxo_filter_clamped.argtypes = [u8p, u32, u32, u32, C.c_void_p, C.c_int, u32, u32, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -190,3 +191,21 @@ def local_maxima(xs, ys, scores, radius) -> list[int]:
     out = np.empty(max(len(xs), 1), np.uint32)
     n = lib().nxo_local_maxima(_p(xs), _p(ys), _p(sc), len(xs), int(radius), _p(out))
     return [int(i) for i in out[:n]]
+
+
+FILTER_OUT = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.int16): 5, np.dtype(np.int32): 6,
+              np.dtype(np.float32): 8}
+
+
+def filter_clamped(image, kernel, out_dtype) -> np.ndarray:
+    """filter_clamped (src/filter/mod.rs:29-70, :202-212) of an (H, W) or (H, W, C)
+    u8 image by a 2-D f32 or i32 kernel, clamped to out_dtype."""
+    a = np.ascontiguousarray(image, np.uint8)
+    k = np.ascontiguousarray(kernel)
+    H, W = a.shape[:2]
+    ch = 1 if a.ndim == 2 else a.shape[2]
+    kt = 0 if k.dtype == np.float32 else 1
+    od = np.dtype(out_dtype)
+    out = np.zeros(a.shape, od)
+    lib().nxo_filter_clamped(_p(a), W, H, ch, _p(k), kt, k.shape[1], k.shape[0], FILTER_OUT[od], _p(out))
+    return out

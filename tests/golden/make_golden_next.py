@@ -1,8 +1,9 @@
 """Extract the reference's known-answer tests for integral images and
 non-maximum suppression as fixtures.
 
-Reads imageproc's ``src/integral_image.rs`` (tests :471-567) and
-``src/suppress.rs`` (tests :209-270) as TEXT and writes
+Reads imageproc's ``src/integral_image.rs`` (tests :471-567),
+``src/suppress.rs`` (tests :209-270) and ``src/filter/mod.rs`` (tests
+:479-513, :615-693) as TEXT and writes
 ``reference_next_tests.json`` beside this script. Nothing of the reference is
 compiled or run: the ``gray_image!`` / ``rgb_image!`` literals, the
 ``sum_image_pixels`` assertions, the ``put_pixel`` calls and the ``T::new``
@@ -107,6 +108,45 @@ def suppress_tests(src: str) -> list[dict]:
     return cases
 
 
+def filter_tests(src: str) -> list[dict]:
+    """filter_clamped's known answers: the Sobel test (i32 kernel -> i16) and the
+    horizontal / vertical 1/3 box tests, which are filter_clamped with 1 x 3 and
+    3 x 1 f32 kernels into u8."""
+    cases = []
+    body, line = test_body(src, "test_filter_clamped_with_results_outside_input_channel_range")
+    kbody = body[body.index("Kernel::new(&[") + len("Kernel::new(&["):]
+    kvals = [int(v) for v in kbody[:kbody.index("]")].replace("\n", " ").split(",") if v.strip()]
+    kw, kh = (int(v) for v in re.search(r"\],\s*(\d+),\s*(\d+)\)", kbody).groups())
+    img, end = macro_body(body, "gray_image")
+    exp, _ = macro_body(body, "gray_image", end)
+    cases.append({"name": "test_filter_clamped_with_results_outside_input_channel_range", "line": line,
+                  "kernel_type": "i32", "kernel": kvals, "kernel_width": kw, "kernel_height": kh,
+                  "image": parse_image(img), "expected": parse_image(exp)})
+    for name, horizontal in (("test_horizontal_filter", True), ("test_vertical_filter", False)):
+        body, line = test_body(src, name)
+        img, end = macro_body(body, "gray_image")
+        exp, _ = macro_body(body, "gray_image", end)
+        m = re.search(r"\[1f32 / (\d+)f32; (\d+)\]", body)
+        n = int(m.group(2))
+        cases.append({"name": name, "line": line, "kernel_type": "f32", "kernel_one_over": int(m.group(1)),
+                      "kernel_width": n if horizontal else 1, "kernel_height": 1 if horizontal else n,
+                      "image": parse_image(img), "expected": parse_image(exp)})
+    # separable_filter_equal = vertical_filter(horizontal_filter(.)) with a 3-tap kernel
+    for name in ("test_separable_filter", "test_separable_filter_integer_kernel"):
+        body, line = test_body(src, name)
+        img, end = macro_body(body, "gray_image")
+        exp, _ = macro_body(body, "gray_image", end)
+        m = re.search(r"let kernel = \[1(f32 / (\d+)f32|i32); (\d+)\]", body)
+        case = {"name": name, "line": line, "separable": True, "taps": int(m.group(3)),
+                "image": parse_image(img), "expected": parse_image(exp)}
+        if m.group(2):
+            case.update(kernel_type="f32", kernel_one_over=int(m.group(2)))
+        else:
+            case.update(kernel_type="i32", kernel_value=1)
+        cases.append(case)
+    return cases
+
+
 def main() -> None:
     src = Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_SRC
     data = {
@@ -114,6 +154,7 @@ def main() -> None:
         "integral_image": {"file": "src/integral_image.rs",
                            "cases": integral_tests((src / "integral_image.rs").read_text())},
         "suppress": {"file": "src/suppress.rs", "cases": suppress_tests((src / "suppress.rs").read_text())},
+        "filter": {"file": "src/filter/mod.rs", "cases": filter_tests((src / "filter" / "mod.rs").read_text())},
     }
     OUT.write_text(json.dumps(data, indent=1))
     print(f"wrote {OUT}")

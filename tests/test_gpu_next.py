@@ -1,6 +1,7 @@
-"""Integral images and non-maximum suppression on the GPU against the oracle
-(src/integral_image.rs, src/suppress.rs). Bar: bit-exact tables and outputs,
-identical point lists."""
+"""Integral images, non-maximum suppression and filter_clamped on the GPU
+against the oracle (src/integral_image.rs, src/suppress.rs,
+src/filter/mod.rs). Bar: bit-exact tables and outputs, identical point
+lists."""
 
 import json
 from pathlib import Path
@@ -8,6 +9,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+from imageproc_b200 import filter as fl
 from imageproc_b200 import integral_image as ii
 from imageproc_b200 import suppress as sp
 from oracle import oracle as O
@@ -153,3 +155,76 @@ def test_local_maxima_matches_oracle():
             sc[g.integers(0, n, 3)] = np.nan
         r = int(g.integers(0, 8))
         assert sp.local_maxima_indices(xs, ys, sc, r) == O.local_maxima(xs, ys, sc, r), trial
+
+
+# ---- filter_clamped -----------------------------------------------------------------
+
+F32_OUTS = [np.uint8, np.uint16, np.float32]
+I32_OUTS = [np.uint8, np.uint16, np.int16, np.int32]
+
+
+def _same(got, exp):
+    # bit-exact, except that a NaN is any NaN: the GPU writes its canonical NaN
+    # where x86 propagates the kernel's NaN payload
+    if got.dtype == np.float32:
+        nan = np.isnan(exp)
+        return np.array_equal(np.isnan(got), nan) and np.array_equal(got[~nan].view(np.uint32),
+                                                                      exp[~nan].view(np.uint32))
+    return np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("channels", [1, 3, 4])
+def test_filter_clamped_matches_oracle(channels):
+    g = np.random.default_rng(channels)
+    for trial in range(24):
+        H, W = int(g.integers(1, 70)), int(g.integers(1, 90))
+        img = g.integers(0, 256, (H, W) if channels == 1 else (H, W, channels), dtype=np.uint8)
+        kh, kw = int(g.integers(1, 9)), int(g.integers(1, 9))  # even and odd sides, some wider than the image
+        if trial % 2:
+            k = (g.standard_normal((kh, kw)) * 3).astype(np.float32)
+            if trial % 6 == 1:
+                k[0, 0] = np.nan
+            outs = F32_OUTS
+        else:
+            k = g.integers(-2**20, 2**20, (kh, kw)).astype(np.int32)  # sums wrap in i32
+            outs = I32_OUTS
+        for od in outs:
+            got = fl.filter_clamped(img, k, od)
+            exp = O.filter_clamped(img, k, od)
+            assert _same(got, exp), (trial, od, kh, kw)
+
+
+def test_filter_large_kernel_and_image():
+    g = np.random.default_rng(9)
+    img = g.integers(0, 256, (300, 420), dtype=np.uint8)
+    k = g.random((3, 70), dtype=np.float32) / 100  # wider than the shared-memory tile path takes
+    assert np.array_equal(fl.filter_clamped(img, k, np.float32).view(np.uint32),
+                          O.filter_clamped(img, k, np.float32).view(np.uint32))
+    big = g.integers(0, 256, (1080, 1920), dtype=np.uint8)
+    k5 = g.random((5, 5), dtype=np.float32) / 5
+    assert np.array_equal(fl.filter_clamped(big, k5, np.uint8), O.filter_clamped(big, k5, np.uint8))
+
+
+def test_filter_golden_and_forms():
+    for c in GOLDEN["filter"]["cases"]:
+        img = np.array(c["image"]["rows"], np.uint8)
+        exp = np.array(c["expected"]["rows"])
+        if c.get("separable"):
+            k = (np.full(c["taps"], np.float32(1) / np.float32(c["kernel_one_over"]), np.float32)
+                 if c["kernel_type"] == "f32" else np.full(c["taps"], c["kernel_value"], np.int32))
+            got = fl.separable_filter_equal(img, k)
+        elif c["kernel_type"] == "i32":
+            k = np.array(c["kernel"], np.int32).reshape(c["kernel_height"], c["kernel_width"])
+            got = fl.filter_clamped(img, k, np.int16)
+        else:
+            k = np.full(3, np.float32(1) / np.float32(c["kernel_one_over"]), np.float32)
+            got = fl.horizontal_filter(img, k) if c["kernel_height"] == 1 else fl.vertical_filter(img, k)
+        assert np.array_equal(got, exp), c["name"]
+    img = np.array([[1, 2, 3], [4, 5, 6], [7, 8, 9]], np.uint8)
+    assert np.array_equal(fl.laplacian_filter(img), O.filter_clamped(img, fl.LAPLACIAN, np.int16))
+    with pytest.raises(fl.Panic, match="^width and height must be non-zero$"):
+        fl.filter_clamped(img, np.zeros((0, 3), np.float32))
+    with pytest.raises(fl.Panic, match="^the two 1D kernels must be the same length$"):
+        fl.separable_filter(img, np.ones(3, np.float32), np.ones(5, np.float32))
+    with pytest.raises(ValueError):
+        fl.filter_clamped(img, np.ones((3, 3), np.float32), np.int16)  # no Clamp<f32> for i16

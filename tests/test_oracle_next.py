@@ -96,3 +96,44 @@ def test_local_maxima_golden():
     pts = c["points"]
     idx = O.local_maxima([p[0] for p in pts], [p[1] for p in pts], [p[2] for p in pts], c["radius"])
     assert [pts[i] for i in idx] == c["expected"]
+
+
+# ---- filter_clamped (src/filter/mod.rs) -------------------------------------
+
+def golden_kernel(c):
+    if c["kernel_type"] == "i32":
+        if "kernel" in c:
+            return np.array(c["kernel"], np.int32).reshape(c["kernel_height"], c["kernel_width"])
+        return np.full(c["taps"], c["kernel_value"], np.int32)
+    k = np.float32(1) / np.float32(c["kernel_one_over"])
+    if c.get("separable"):
+        return np.full(c["taps"], k, np.float32)
+    return np.full((c["kernel_height"], c["kernel_width"]), k, np.float32)
+
+
+def oracle_golden_filter(c):
+    img = np.array(c["image"]["rows"], np.uint8)
+    k = golden_kernel(c)
+    if c.get("separable"):
+        h = O.filter_clamped(img, k.reshape(1, -1), np.uint8)
+        return O.filter_clamped(h, k.reshape(-1, 1), np.uint8)
+    od = {"i16": np.int16, "u8": np.uint8}[c["expected"]["type"]]
+    return O.filter_clamped(img, k, od)
+
+
+@pytest.mark.parametrize("name", [c["name"] for c in GOLDEN["filter"]["cases"]])
+def test_filter_golden(name):
+    c = case("filter", name)
+    exp = np.array(c["expected"]["rows"])
+    assert np.array_equal(oracle_golden_filter(c), exp)
+
+
+def test_filter_clamp_rules():
+    img = np.array([[10, 20], [30, 40]], np.uint8)
+    # NaN accumulators clamp to the maximum, negatives to the minimum
+    k = np.array([[np.nan]], np.float32)
+    assert (O.filter_clamped(img, k, np.uint8) == 255).all()
+    assert (O.filter_clamped(img, -np.ones((1, 1), np.float32), np.uint16) == 0).all()
+    big = np.full((1, 1), 2**30, np.int32)  # wraps in i32, then clamps
+    got = O.filter_clamped(img, big, np.int32)
+    assert got[0, 0] == -2**31  # 10 * 2^30 = 2^33 + 2^31 wraps to 2^31, i.e. -2^31 as i32
