@@ -124,6 +124,17 @@ int path_from_env() {
 }
 std::atomic<int> g_path{path_from_env()};
 
+// Row bands of the host-buffer match calls: 0 = choose from the map's size,
+// n >= 1 = n bands (tuning).
+int bands_from_env() {
+  const char* v = std::getenv("IPB_HOST_BANDS");
+  if (!v) return 0;
+  const int n = std::atoi(v);
+  return n < 0 ? 0 : n;
+}
+const int g_host_bands = bands_from_env();
+constexpr uint32_t kMaxBands = 16;
+
 ipb_status fail(ipb_status st, const std::string& msg) {
   g_last_error = msg;
   return st;
@@ -159,10 +170,22 @@ struct Context {
   unsigned int tag = 0;            // tag of the last tensor-core launch
   unsigned int tag_checked = 0;    // largest failing tag already reported
   bool tensor_since_check = false;
+  // copy streams of the banded host calls: image rows in, score rows out
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t band_in[kMaxBands] = {}, band_done[kMaxBands] = {}, out_done = nullptr;
   ~Context() {
     if (device < 0) return;
     cudaSetDevice(device);
     if (last) cudaEventSynchronize(last);
+    for (cudaStream_t s : {s_in, s_out})
+      if (s) cudaStreamSynchronize(s);
+    for (uint32_t b = 0; b < kMaxBands; ++b) {
+      if (band_in[b]) cudaEventDestroy(band_in[b]);
+      if (band_done[b]) cudaEventDestroy(band_done[b]);
+    }
+    if (out_done) cudaEventDestroy(out_done);
+    for (cudaStream_t s : {s_in, s_out})
+      if (s) cudaStreamDestroy(s);
     for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys})
       if (b->p) cudaFree(b->p);
     if (pinned) cudaFreeHost(pinned);
@@ -293,6 +316,87 @@ ipb_status run_match(Context* c, const MatchArgs& a) {
   return IPB_OK;
 }
 
+// How many row bands a host-buffer match is cut into. One call moves the
+// image in, computes and moves the map out; in bands the three overlap (image
+// rows of band b+1 cross PCIe while band b is scored and band b-1's scores
+// come back), so the call costs about its larger copy instead of the sum.
+// A map below 2 MiB is one band: its copies are shorter than a launch.
+uint32_t host_bands(size_t out_bytes, uint32_t Ho, uint32_t w, uint32_t h) {
+  if (w == 0 || h == 0) return 1;
+  uint32_t n = g_host_bands > 0 ? (uint32_t)g_host_bands : (out_bytes >= (4u << 20) ? 4u : out_bytes >= (2u << 20) ? 2u : 1u);
+  n = std::min(n, kMaxBands);
+  return std::min(n, (Ho + 15) / 16);  // bands of at least 16 score rows
+}
+
+ipb_status ensure_band_streams(Context* c) {
+  for (cudaStream_t* s : {&c->s_in, &c->s_out})
+    if (!*s) IPB_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (uint32_t b = 0; b < kMaxBands; ++b) {
+    if (!c->band_in[b]) IPB_CUDA(cudaEventCreateWithFlags(&c->band_in[b], cudaEventDisableTiming), "cudaEventCreate");
+    if (!c->band_done[b])
+      IPB_CUDA(cudaEventCreateWithFlags(&c->band_done[b], cudaEventDisableTiming), "cudaEventCreate");
+  }
+  if (!c->out_done) IPB_CUDA(cudaEventCreateWithFlags(&c->out_done, cudaEventDisableTiming), "cudaEventCreate");
+  return IPB_OK;
+}
+
+// The host-buffer match in nb row bands. Band b scores rows [o0, o1) of the
+// map from image rows [o0, o1 + h - 1): a problem of its own whose output
+// rows keep the full map's pitch, so every score is the one the whole-map
+// launch writes. Image rows cross once, in order (a band copies only the rows
+// the previous band did not); bands start on multiples of 16 rows so a
+// 16-byte-aligned image stays aligned.
+ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* image, const uint8_t* tpl,
+                             const uint8_t* mask, uint32_t nb, float* out) {
+  ipb_status st;
+  if ((st = ensure_band_streams(c))) return st;
+  const uint32_t W = full.W, Wo = full.W - full.w + 1, Ho = full.H - full.h + 1;
+  const size_t tb = (size_t)full.w * full.h;
+  const uint32_t rows = (uint32_t)align_up((Ho + nb - 1) / nb, 16);
+  uint8_t* d_img = static_cast<uint8_t*>(c->img.p);
+  auto enqueue = [&]() -> ipb_status {
+    IPB_CUDA(cudaStreamWaitEvent(c->s_in, c->last, 0), "cudaStreamWaitEvent");
+    IPB_CUDA(cudaMemcpyAsync(c->tpl.p, tpl, tb, cudaMemcpyHostToDevice, c->s_in), "copy template");
+    if (mask) IPB_CUDA(cudaMemcpyAsync(c->mask.p, mask, tb, cudaMemcpyHostToDevice, c->s_in), "copy mask");
+    uint32_t have = 0, bands = 0;  // image rows on the device, bands queued
+    for (uint32_t o0 = 0; o0 < Ho; o0 += rows, ++bands) {
+      const uint32_t o1 = std::min(Ho, o0 + rows), need = o1 + full.h - 1;
+      IPB_CUDA(cudaMemcpyAsync(d_img + (size_t)have * W, image + (size_t)have * W, (size_t)(need - have) * W,
+                               cudaMemcpyHostToDevice, c->s_in),
+               "copy image rows");
+      have = need;
+      IPB_CUDA(cudaEventRecord(c->band_in[bands], c->s_in), "cudaEventRecord");
+      IPB_CUDA(cudaStreamWaitEvent(c->stream, c->band_in[bands], 0), "cudaStreamWaitEvent");
+      MatchArgs a = full;
+      a.img = full.img + (size_t)o0 * W;
+      a.H = need - o0;
+      a.out = full.out + (size_t)o0 * Wo;
+      ipb_status s2 = run_match(c, a);
+      if (s2) return s2;
+      IPB_CUDA(cudaEventRecord(c->band_done[bands], c->stream), "cudaEventRecord");
+    }
+    // queued after every launch: a copy to pageable memory blocks the host
+    for (uint32_t b = 0; b < bands; ++b) {
+      const uint32_t o0 = b * rows, o1 = std::min(Ho, o0 + rows);
+      IPB_CUDA(cudaStreamWaitEvent(c->s_out, c->band_done[b], 0), "cudaStreamWaitEvent");
+      IPB_CUDA(cudaMemcpyAsync(out + (size_t)o0 * Wo, full.out + (size_t)o0 * Wo, (size_t)(o1 - o0) * Wo * sizeof(float),
+                               cudaMemcpyDeviceToHost, c->s_out),
+               "copy score rows");
+    }
+    IPB_CUDA(cudaEventRecord(c->out_done, c->s_out), "cudaEventRecord");
+    IPB_CUDA(cudaStreamWaitEvent(c->stream, c->out_done, 0), "cudaStreamWaitEvent");
+    return IPB_OK;
+  };
+  if ((st = enqueue())) {
+    // nothing may touch the caller's buffers after the call returns
+    cudaStreamSynchronize(c->s_in);
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->s_out);
+    return st;
+  }
+  return finish_sync(c, c->stream);
+}
+
 ipb_status host_match(const uint8_t* image, uint32_t W, uint32_t H, const uint8_t* tpl, uint32_t w,
                       uint32_t h, int method, const uint8_t* mask, uint32_t mw, uint32_t mh,
                       float* out) {
@@ -307,15 +411,17 @@ ipb_status host_match(const uint8_t* image, uint32_t W, uint32_t H, const uint8_
   if ((st = ensure(c, c->img, ib)) || (st = ensure(c, c->tpl, tb)) || (st = ensure(c, c->out, ob)))
     return st;
   if (mask && (st = ensure(c, c->mask, tb))) return st;
+  MatchArgs a{static_cast<const uint8_t*>(c->img.p), W, H, static_cast<const uint8_t*>(c->tpl.p), w, h,
+              mask ? static_cast<const uint8_t*>(c->mask.p) : nullptr,
+              mask ? host_mask_is_binary(mask, tb) : false, method, g_precision.load(),
+              static_cast<float*>(c->out.p), c->stream};
+  const uint32_t nb = host_bands(ob, H - h + 1, w, h);
+  if (nb > 1) return host_match_banded(c, a, image, tpl, mask, nb, out);
   IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
   if (ib) IPB_CUDA(cudaMemcpyAsync(c->img.p, image, ib, cudaMemcpyHostToDevice, c->stream), "copy image");
   if (tb) IPB_CUDA(cudaMemcpyAsync(c->tpl.p, tpl, tb, cudaMemcpyHostToDevice, c->stream), "copy template");
   if (mask && tb)
     IPB_CUDA(cudaMemcpyAsync(c->mask.p, mask, tb, cudaMemcpyHostToDevice, c->stream), "copy mask");
-  MatchArgs a{static_cast<const uint8_t*>(c->img.p), W, H, static_cast<const uint8_t*>(c->tpl.p), w, h,
-              mask ? static_cast<const uint8_t*>(c->mask.p) : nullptr,
-              mask ? host_mask_is_binary(mask, tb) : false, method, g_precision.load(),
-              static_cast<float*>(c->out.p), c->stream};
   if ((st = run_match(c, a))) return st;
   IPB_CUDA(cudaMemcpyAsync(out, c->out.p, ob, cudaMemcpyDeviceToHost, c->stream), "copy scores");
   return finish_sync(c, c->stream);

@@ -114,8 +114,20 @@ __global__ void __launch_bounds__(32 * kSegs) sat_cols_kernel(uint32_t cols, uin
   T run = 0;
   for (int k = 0; k < segi; ++k) run += s_tot[k][threadIdx.x & 31];
   if (col < cols) {
-#pragma unroll 8
-    for (uint32_t r = r0; r < r1; ++r) {
+    // eight rows loaded before any is stored, so the reads overlap instead of
+    // waiting on each other through the stores
+    uint32_t r = r0;
+    for (; r + 8 <= r1; r += 8) {
+      T v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = sat[(size_t)(r + k) * cols + col];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        run += v[k];
+        sat[(size_t)(r + k) * cols + col] = run;
+      }
+    }
+    for (; r < r1; ++r) {
       T* p = sat + (size_t)r * cols + col;
       run += *p;
       *p = run;
