@@ -47,8 +47,10 @@ roofline (algorithmic bytes: input read once, output written once) with the
 oracle's single-thread C restatement of the reference timed on the same
 input: integral_squared_image (u64) of a 4096x4096 scene,
 suppress_non_maximum (radius 8) of a 4065x4065 f32 score map,
-filter_clamped (5x5 f32 kernel) of the 4096x4096 scene into u8, and
-local_maxima (radius 8) of 100k scored points.
+filter_clamped (5x5 f32 kernel) of the 4096x4096 scene into u8,
+local_maxima (radius 8) of 100k scored points, and the example workflow of
+examples/template_matching.rs (crop, two score maps, rescale, pad, draw) on
+the 1080p scene through its host entry point.
 """
 
 from __future__ import annotations
@@ -373,7 +375,8 @@ def run_side_configs(args, world, rank, local) -> dict:
 
 
 def run_next_rows(args, world, rank, local) -> dict:
-    """Integral image, non-maximum suppression, filter_clamped and local maxima."""
+    """Integral image, non-maximum suppression, filter_clamped, local maxima and the
+    example workflow."""
     import ctypes as C
 
     import torch
@@ -485,6 +488,30 @@ def run_next_rows(args, world, rank, local) -> dict:
         "api": "ipb_local_maxima (host arrays in and out, copies inside the time)",
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "all points, oracle restatement of src/suppress.rs:111-173"}}
+
+    # the example workflow of examples/template_matching.rs on the 1080p scene:
+    # crop, two score maps, rescale, pad, draw (PNG coding excluded on both sides)
+    from imageproc_b200.examples import template_matching as ex
+    scene, _, _, _ = synthetic.blob_scene()
+    roi = (900, 500, 64, 64)
+    for _ in range(3):
+        ex.run_pipeline(scene, *roi)
+    t0 = time.perf_counter()
+    for _ in range(10):
+        ex.run_pipeline(scene, *roi)
+    ms = max_over_ranks((time.perf_counter() - t0) / 10 * 1e3, world)
+    threads = O.default_threads()
+    t0 = time.perf_counter()
+    O.template_matching_example(scene, *roi)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    res["example_template_matching"] = {
+        "workload": "blob_scene 1920x1080 u8, template = 64x64 crop at (900, 500): template, outlined image, "
+                    "SSE and SSE-normalised maps rescaled, padded and outlined (4 images)",
+        "ms": ms, "api": "ipb_example_template_matching (host image in, host images out, copies inside the time)",
+        "cpu_baseline": {"ms": cpu_ms, "cores": threads, "kind": "port",
+                         "sample": "the whole workflow: oracle exact score maps over "
+                                   f"{threads} threads, numpy rescale and drawing "
+                                   "(examples/template_matching.rs:63-134)"}}
     return res
 
 

@@ -91,7 +91,8 @@ void note_timed(KernelTimer* t, double macs, double bytes) {
 const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
-      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress", "filter"};
+      "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress", "filter",
+      "example"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -167,6 +168,7 @@ struct Context {
   void* pinned = nullptr;  // small pinned host block: reduction results, error words
   DevBuf errw;                     // tensor-core error word (largest failing launch tag)
   DevBuf many_keys;                // per-template extremes keys of the many-templates path
+  DevBuf rgb, keys;                // the example workflow: RGB canvas, score-map range
   unsigned int tag = 0;            // tag of the last tensor-core launch
   unsigned int tag_checked = 0;    // largest failing tag already reported
   bool tensor_since_check = false;
@@ -186,7 +188,7 @@ struct Context {
     if (out_done) cudaEventDestroy(out_done);
     for (cudaStream_t s : {s_in, s_out})
       if (s) cudaStreamDestroy(s);
-    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys})
+    for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys, &rgb, &keys})
       if (b->p) cudaFree(b->p);
     if (pinned) cudaFreeHost(pinned);
     if (last) cudaEventDestroy(last);
@@ -857,6 +859,57 @@ IPB_API ipb_status ipb_filter_clamped_device(const uint8_t* d_image, uint32_t W,
                          static_cast<cudaStream_t>(stream)),
            "filter launch");
   return IPB_OK;
+}
+
+IPB_API ipb_status ipb_example_template_matching(const uint8_t* image, uint32_t W, uint32_t H, uint32_t tx,
+                                                 uint32_t ty, uint32_t tw, uint32_t th, uint8_t* template_out,
+                                                 uint8_t* image_rgb, uint8_t* sse_rgb, uint8_t* sse_norm_rgb) {
+  // copy_sub_image's assertion (examples/template_matching.rs:79-82), in u64
+  // so that no sum wraps
+  if (!((uint64_t)tx + tw < W && (uint64_t)ty + th < H)) return fail(IPB_ERR_INVALID_ARGUMENT, "invalid sub-image");
+  if (!tw || !th)
+    return fail(IPB_ERR_INVALID_ARGUMENT,
+                "an empty template's score map does not fit the padded canvas (the reference's copy_from "
+                "fails with a dimension mismatch)");
+  if (!image || !template_out || !image_rgb || !sse_rgb || !sse_norm_rgb)
+    return fail(IPB_ERR_INVALID_ARGUMENT, "null buffer");
+  Context* c = nullptr;
+  ipb_status st;
+  if ((st = get_ctx(&c))) return st;
+  const size_t ib = (size_t)W * H, tb = (size_t)tw * th, rb = 3 * ib;
+  const uint32_t Wo = W - tw + 1, Ho = H - th + 1;
+  const size_t ob = (size_t)Wo * Ho * sizeof(float);
+  if ((st = ensure(c, c->img, ib)) || (st = ensure(c, c->tpl, tb)) || (st = ensure(c, c->out, ob)) ||
+      (st = ensure(c, c->rgb, rb)) || (st = ensure(c, c->keys, 2 * sizeof(uint32_t))))
+    return st;
+  cudaStream_t s = c->stream;
+  const uint8_t* d_img = static_cast<const uint8_t*>(c->img.p);
+  uint8_t* d_tpl = static_cast<uint8_t*>(c->tpl.p);
+  uint8_t* d_rgb = static_cast<uint8_t*>(c->rgb.p);
+  uint32_t* d_keys = static_cast<uint32_t*>(c->keys.p);
+  // roi = Rect::at(tx as i32, ty as i32).of_size(tw, th): right/bottom inclusive
+  const int32_t left = (int32_t)tx, top = (int32_t)ty;
+  const int32_t right = left + (int32_t)tw - 1, bottom = top + (int32_t)th - 1;
+  IPB_CUDA(cudaStreamWaitEvent(s, c->last, 0), "cudaStreamWaitEvent");
+  IPB_CUDA(cudaMemcpyAsync(c->img.p, image, ib, cudaMemcpyHostToDevice, s), "copy image");
+  IPB_CUDA(launch_crop(d_img, W, tx, ty, tw, th, d_tpl, s), "copy_sub_image");
+  IPB_CUDA(cudaMemcpyAsync(template_out, d_tpl, tb, cudaMemcpyDeviceToHost, s), "copy template");
+  IPB_CUDA(launch_render(d_img, nullptr, 0, 0, 0, 0, nullptr, W, H, left, top, right, bottom, d_rgb, s),
+           "draw_green_rect");
+  IPB_CUDA(cudaMemcpyAsync(image_rgb, d_rgb, rb, cudaMemcpyDeviceToHost, s), "copy image with roi");
+  const int methods[2] = {IPB_SUM_OF_SQUARED_ERRORS, IPB_SUM_OF_SQUARED_ERRORS_NORMALIZED};
+  uint8_t* outs[2] = {sse_rgb, sse_norm_rgb};
+  for (int k = 0; k < 2; ++k) {
+    MatchArgs a{d_img, W, H, d_tpl, tw, th, nullptr, false, methods[k], g_precision.load(),
+                static_cast<float*>(c->out.p), s};
+    if ((st = run_match(c, a))) return st;
+    IPB_CUDA(launch_map_range(static_cast<const float*>(c->out.p), (size_t)Wo * Ho, d_keys, s), "score range");
+    IPB_CUDA(launch_render(nullptr, static_cast<const float*>(c->out.p), Wo, Ho, tw / 2, th / 2, d_keys, W, H,
+                           left, top, right, bottom, d_rgb, s),
+             "rescale, pad and draw");
+    IPB_CUDA(cudaMemcpyAsync(outs[k], d_rgb, rb, cudaMemcpyDeviceToHost, s), "copy result");
+  }
+  return finish_sync(c, s);
 }
 
 IPB_API ipb_status ipb_match_template_device(const uint8_t* d_image, uint32_t W, uint32_t H,

@@ -23,6 +23,7 @@ enum KernelId : int {
   kKernelMany,
   kKernelSuppress,
   kKernelFilter,
+  kKernelExample,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -111,6 +112,17 @@ bool filter_types_supported(int ktype, int otype);
 // kw x kh row-major kernel (device memory); out is W x H x channels of otype.
 cudaError_t launch_filter(const uint8_t* img, uint32_t W, uint32_t H, uint32_t channels, const void* kern, int ktype,
                           uint32_t kw, uint32_t kh, int otype, void* out, cudaStream_t s);
+
+// ---- the example workflow of examples/template_matching.rs (tm_example.cu) ---
+cudaError_t launch_crop(const uint8_t* img, uint32_t W, uint32_t x, uint32_t y, uint32_t w, uint32_t h,
+                        uint8_t* out, cudaStream_t s);
+// keys[0..1] <- order keys of the map's min and max, NaN skipped
+cudaError_t launch_map_range(const float* map, size_t n, uint32_t* keys, cudaStream_t s);
+// W x H x 3 RGB: the gray image (gray != null) or the map rescaled to u8 over
+// keys' range and placed at (px, py), with the rectangle outline in green
+cudaError_t launch_render(const uint8_t* gray, const float* map, uint32_t Wo, uint32_t Ho, uint32_t px,
+                          uint32_t py, const uint32_t* keys, uint32_t W, uint32_t H, int32_t left, int32_t top,
+                          int32_t right, int32_t bottom, uint8_t* rgb, cudaStream_t s);
 
 // ---- CUDA-core exact kernel (tm_exact_cc.cu) ------------------------------
 size_t exact_cc_scratch_bytes(const MatchArgs& a);

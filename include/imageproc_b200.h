@@ -409,6 +409,27 @@ ipb_status ipb_filter_clamped_device(const uint8_t *d_image, uint32_t width, uin
                                      uint32_t kernel_width, uint32_t kernel_height, int out_type,
                                      void *d_out, void *stream);
 
+/* ---- the example workflow ----------------------------------------------------------
+ * What examples/template_matching.rs main (:136-190) computes after decoding
+ * its input, as one device pipeline over a width x height Luma image:
+ *   template_out  (tw x th)   copy_sub_image(image, tx, ty, tw, th) (:78-92),
+ *                             which asserts tx + tw < width and ty + th < height
+ *                             ("invalid sub-image");
+ *   image_rgb     (W x H x 3) draw_green_rect(image, roi) (:94-98): the image
+ *                             as RGB with the outline of roi = Rect::at(tx, ty)
+ *                             .of_size(tw, th) in (0, 255, 0);
+ *   sse_rgb, sse_norm_rgb     run_match_template (:100-134) for
+ *                             SumOfSquaredErrors and its normalised form: the
+ *                             score map (at the library's precision) rescaled
+ *                             to u8 by convert_to_gray_image (:63-76), placed in
+ *                             a W x H canvas at (tw/2, th/2), drawn with roi.
+ * The example's `parallel` argument selects match_template_parallel, whose
+ * scores are identical; it has no counterpart here. tw and th must be non-zero
+ * (the reference fails placing an empty template's map: a dimension mismatch). */
+ipb_status ipb_example_template_matching(const uint8_t *image, uint32_t width, uint32_t height, uint32_t tx,
+                                         uint32_t ty, uint32_t tw, uint32_t th, uint8_t *template_out,
+                                         uint8_t *image_rgb, uint8_t *sse_rgb, uint8_t *sse_norm_rgb);
+
 #ifdef __cplusplus
 }
 #endif

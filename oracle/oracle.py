@@ -209,3 +209,63 @@ def filter_clamped(image, kernel, out_dtype) -> np.ndarray:
     out = np.zeros(a.shape, od)
     lib().nxo_filter_clamped(_p(a), W, H, ch, _p(k), kt, k.shape[1], k.shape[0], FILTER_OUT[od], _p(out))
     return out
+
+
+# ---- the example workflow: examples/template_matching.rs -------------------------
+
+def convert_to_gray_image(scores) -> np.ndarray:
+    """convert_to_gray_image (examples/template_matching.rs:63-76): lo and hi scanned
+    with `<` / `>` from +inf / -inf (NaN never an extreme), then
+    `(255.0 * (x - lo) / range) as u8` in f32 with Rust's saturating cast."""
+    a = np.asarray(scores, np.float32)
+    finite = a[~np.isnan(a)]
+    lo = finite.min() if finite.size else np.float32(np.inf)
+    hi = finite.max() if finite.size else np.float32(-np.inf)
+    rng = np.float32(hi - lo)
+    with np.errstate(all="ignore"):
+        s = (np.float32(255.0) * (a - np.float32(lo))) / rng
+        return np.where(np.isnan(s), 0, np.clip(np.trunc(s), 0, 255)).astype(np.uint8)
+
+
+def draw_green_rect(gray, left, top, width, height) -> np.ndarray:
+    """draw_green_rect (examples/template_matching.rs:94-98): the gray image as RGB
+    with the outline of Rect::at(left, top).of_size(width, height) in (0, 255, 0):
+    draw_hollow_rect_mut (src/drawing/rect.rs:22-35) draws the four edges, each
+    an axis-aligned line segment whose pixels outside the image are skipped
+    (src/drawing/line.rs:183-200)."""
+    g = np.asarray(gray, np.uint8)
+    H, W = g.shape
+    rgb = np.repeat(g[:, :, None], 3, axis=2)
+    right, bottom = left + width - 1, top + height - 1
+    green = np.array([0, 255, 0], np.uint8)
+    xs = range(max(left, 0), min(right, W - 1) + 1)
+    ys = range(max(top, 0), min(bottom, H - 1) + 1)
+    for yy in (top, bottom):
+        if 0 <= yy < H:
+            for xx in xs:
+                rgb[yy, xx] = green
+    for xx in (left, right):
+        if 0 <= xx < W:
+            for yy in ys:
+                rgb[yy, xx] = green
+    return rgb
+
+
+def template_matching_example(image, x, y, w, h, precision=0) -> dict:
+    """What examples/template_matching.rs main (:136-190) computes after decoding:
+    the template, the outlined image and the two outlined, rescaled, padded
+    score maps (run_match_template :100-134), with the oracle's scores at the
+    given precision (0 exact FP64, 1 exact f32, 2 the reference's f32)."""
+    a = np.ascontiguousarray(image, np.uint8)
+    H, W = a.shape
+    assert x + w < W and y + h < H, "invalid sub-image"
+    template = a[y:y + h, x:x + w].copy()
+    out = {"template": template, "image": draw_green_rect(a, x, y, w, h)}
+    for name, method in (("result_sse", 0), ("result_sse_norm", 1)):
+        scores = (match_reference(a, template, method) if precision == 2
+                  else match_exact(a, template, method, precision=precision))
+        scaled = convert_to_gray_image(scores)
+        padded = np.zeros((H, W), np.uint8)
+        padded[h // 2:h // 2 + scaled.shape[0], w // 2:w // 2 + scaled.shape[1]] = scaled
+        out[name] = draw_green_rect(padded, x, y, w, h)
+    return out
