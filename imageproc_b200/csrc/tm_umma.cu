@@ -64,7 +64,9 @@ constexpr int kStages = 2;  // A-row stages in tensor memory
 constexpr uint32_t kMaxRps = 16;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 2000000000ull;
-constexpr uint32_t kSmemHeader = 1024;
+constexpr uint32_t kBandTable = 1024;          // per-row MMA band table (uint4 per image row)
+constexpr uint32_t kMaxTileRows = 256;         // NT + h - 1 <= 128 + 128 - 1
+constexpr uint32_t kSmemHeader = kBandTable + kMaxTileRows * 16;
 constexpr uint32_t kMinSmem = 120 * 1024;  // keeps residency at one CTA per SM
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
@@ -310,7 +312,6 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   const uint32_t tmem = *s_tmem;
   const uint32_t a_col0 = NCORR * L.NT;
   const uint32_t a_row_cols = NPL * KS;
-  const uint32_t idesc0 = idesc_u8u8_s32(kM, 16) & ~(0x3Fu << 17);
 
   uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
   uint32_t tcount = 0;       // tiles finished by this CTA
@@ -368,6 +369,16 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         }
         *reinterpret_cast<uint4*>(zbuf + zp * zplane + (size_t)(c * q.zrows + j) * 16) =
             make_uint4(wd[0], wd[1], wd[2], wd[3]);
+      }
+      // the MMA band of every image row r of a tile: image row r feeds output
+      // rows n in [r-h+1, r], rounded out to 16 (rows past the map are computed,
+      // not stored): {first accumulator column n0, instruction descriptor with
+      // N = n1 - n0, first Z row of the band}
+      for (uint32_t r = threadIdx.x; r < q.rows_max; r += kThreads) {
+        const uint32_t n0 = (r + 1 > q.h ? r + 1 - q.h : 0u) & ~15u;
+        const uint32_t n1 = min(L.NT, (r & ~15u) + 16u);
+        const uint32_t idesc = (idesc_u8u8_s32(kM, 16) & ~(0x3Fu << 17)) | (((n1 - n0) >> 3) << 17);
+        reinterpret_cast<uint4*>(smem + kBandTable)[r] = make_uint4(n0, idesc, n0 + q.h + 15u - r, 0u);
       }
       // TSS = sum (T*m)^2 (m = 1 unmasked), exact; per-warp partials in shared memory
       unsigned long long t2 = 0;
@@ -494,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t zoff1 = zplane >> 4;
       const uint32_t kstride = 2u * q.zrows;  // one 32-byte K step of Z, in 16-byte units
       const uint32_t ksteps = q.kmma / 32;
-      const uint32_t h = q.h;
+      const uint4* band = reinterpret_cast<const uint4*>(smem + kBandTable);
       const bool leader = elect_one();
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
@@ -506,16 +517,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         tc_fence_after();
         const uint32_t r0 = st * L.rps, cnt = min(nrows, r0 + L.rps) - r0;
         const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
-        // image row r feeds output rows n in [r-h+1, r] of the tile: the band
-        // [n0, n1) rounded out to 16 (rows past the map are computed, not stored)
 #pragma unroll 4
         for (uint32_t i = 0; i < kMaxRps; ++i) {
           if (i >= cnt) break;
-          const uint32_t r = r0 + i;
-          const uint32_t n0 = (r + 1 > h ? r + 1 - h : 0u) & ~15u;
-          const uint32_t n1 = min(L.NT, (r & ~15u) + 16u);
-          const uint32_t idesc = idesc0 | (((n1 - n0) >> 3) << 17);
-          const uint32_t zrow = dlo + n0 + h + 15u - r;  // first Z row of the band
+          const uint4 bd = band[r0 + i];  // n0, idesc, first Z row of the band
+          const uint32_t n0 = bd.x, idesc = bd.y;
+          const uint32_t zrow = dlo + bd.z;
           const uint32_t a = a_stage + i * a_row_cols;
           if (leader) {
 #pragma unroll
