@@ -393,10 +393,10 @@ def run_next_rows(args, world, rank, local) -> dict:
     pk = peaks()
     res = {}
 
-    def roof(nbytes, ms):
+    def roof(nbytes, ms, traffic_key):
         gbs = nbytes / (ms / 1e3) / 1e9
         return {"bound": "hbm", "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": gbs / pk["hbm_gbs"], "traffic": None}
+                "frac": gbs / pk["hbm_gbs"], "traffic": _traffic(traffic_key)}
 
     # integral_squared_image, u64, 4096 x 4096
     side = 4096
@@ -417,7 +417,8 @@ def run_next_rows(args, world, rank, local) -> dict:
     cpu_ms = (time.perf_counter() - t0) * 1e3
     res["integral_squared_image"] = {
         "workload": f"value_noise {side}x{side} u8 -> ({side}+1)^2 u64 table", "ms": ms,
-        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9, "roofline": roof(nbytes, ms),
+        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9,
+        "roofline": roof(nbytes, ms, "integral_squared_u64_4096"),
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "the whole table, oracle restatement of src/integral_image.rs:98-153"}}
     del d_sat
@@ -441,7 +442,8 @@ def run_next_rows(args, world, rank, local) -> dict:
     cpu_ms = (time.perf_counter() - t0) * 1e3 * (wo / 512)
     res["suppress_non_maximum"] = {
         "workload": f"uniform f32 score map {wo}x{wo}, radius 8", "ms": ms,
-        "gpix_per_s": world * wo * wo / (ms / 1e3) / 1e9, "roofline": roof(2 * 4 * wo * wo, ms),
+        "gpix_per_s": world * wo * wo / (ms / 1e3) / 1e9,
+        "roofline": roof(2 * 4 * wo * wo, ms, "suppress_f32_4065_r8"),
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "512 of 4065 rows, oracle restatement of src/suppress.rs:10-107, scaled by rows"}}
     del d_map, d_nms
@@ -464,7 +466,8 @@ def run_next_rows(args, world, rank, local) -> dict:
     cpu_ms = (time.perf_counter() - t0) * 1e3 * (side / 512)
     res["filter_clamped"] = {
         "workload": f"value_noise {side}x{side} u8, 5x5 f32 kernel, clamped to u8", "ms": ms,
-        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9, "roofline": roof(2 * side * side, ms),
+        "gpix_per_s": world * side * side / (ms / 1e3) / 1e9,
+        "roofline": roof(2 * side * side, ms, "filter_clamped_u8_4096_k5"),
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "512 of 4096 rows, oracle restatement of src/filter/mod.rs:29-70, scaled by rows"}}
     del d_f, d_k
