@@ -76,6 +76,19 @@ def test_integral_device_form():
                                            torch.cuda.current_stream().cuda_stream or None))
     torch.cuda.synchronize()
     assert np.array_equal(d_out.cpu().numpy().view(np.uint64), O.integral_image(img, square=True, bits=64))
+    # Luma: the tiled one-write path, whose carries live in the context's
+    # scratch; two calls in a row on one stream share it
+    stream = torch.cuda.current_stream().cuda_stream or None
+    for H, W in ((300, 512), (1000, 777), (33, 8)):
+        gray = g.integers(0, 256, (H, W), dtype=np.uint8)
+        d_gray = torch.from_numpy(gray).cuda()
+        d32 = torch.empty((H + 1, W + 1), dtype=torch.int32, device="cuda")
+        d64 = torch.empty((H + 1, W + 1), dtype=torch.int64, device="cuda")
+        _lib.check(L.ipb_integral_image_device(d_gray.data_ptr(), W, H, 1, 1, 32, d32.data_ptr(), stream))
+        _lib.check(L.ipb_integral_image_device(d_gray.data_ptr(), W, H, 1, 0, 64, d64.data_ptr(), stream))
+        torch.cuda.synchronize()
+        assert np.array_equal(d32.cpu().numpy().view(np.uint32), O.integral_image(gray, square=True, bits=32))
+        assert np.array_equal(d64.cpu().numpy().view(np.uint64), O.integral_image(gray, square=False, bits=64))
 
 
 # ---- suppress_non_maximum ---------------------------------------------------------
