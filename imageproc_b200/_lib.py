@@ -151,6 +151,8 @@ def lib() -> C.CDLL:
     L.ipb_host_alloc.restype = C.c_void_p
     L.ipb_host_free.argtypes = [C.c_void_p]
     L.ipb_host_free.restype = None
+    L.ipb_host_cache_release.argtypes = []
+    L.ipb_host_cache_release.restype = None
     _lib = L
     return L
 

@@ -552,6 +552,16 @@ IPB_API void ipb_host_free(void* ptr) {
   cudaFreeHost(ptr);
 }
 
+IPB_API void ipb_host_cache_release(void) {
+  std::multimap<size_t, void*> blocks;
+  {
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    blocks.swap(g_host_free);
+    g_host_cached = 0;
+  }
+  for (auto& kv : blocks) cudaFreeHost(kv.second);
+}
+
 IPB_API uint64_t ipb_launch_count(void) { return g_launches.load(); }
 
 IPB_API ipb_status ipb_profile_enable(int enable) {

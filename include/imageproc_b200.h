@@ -111,6 +111,9 @@ const char *ipb_version(void);
  * entry points accept ordinary host memory as well. */
 void *ipb_host_alloc(size_t bytes);
 void ipb_host_free(void *ptr);
+/* Return every cached (freed, unused) block to the driver; blocks still in
+ * use are not affected. */
+void ipb_host_cache_release(void);
 
 /* Process-wide precision used by the reference-shaped entry points (the
  * ones without a precision argument). Default IPB_PRECISION_EXACT_FP64, or

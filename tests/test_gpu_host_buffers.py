@@ -22,9 +22,16 @@ def test_host_alloc_reuses_freed_blocks():
     assert q == p  # the cached block comes back
     L.ipb_host_free(q)
     L.ipb_host_free(None)  # no-op
+    L.ipb_host_cache_release()  # the cached block goes back to the driver
+    r = L.ipb_host_alloc(3 << 20)
+    assert r
+    L.ipb_host_free(r)
 
 
 def test_host_api_scores_come_from_the_cache_and_are_correct():
+    # start from an empty cache: blocks that earlier calls left in it would
+    # otherwise be handed out first
+    _lib.lib().ipb_host_cache_release()
     g = np.random.default_rng(3)
     image = g.integers(0, 256, (300, 400), dtype=np.uint8)
     template = g.integers(0, 256, (24, 20), dtype=np.uint8)
