@@ -737,11 +737,11 @@ ipb_status host_suppress(int type, size_t esize, const void* image, uint32_t W, 
   ipb_status st;
   if ((st = get_ctx(&c))) return st;
   if ((st = ensure(c, c->img, bytes)) || (st = ensure(c, c->out, bytes)) ||
-      (st = ensure(c, c->scratch, (size_t)W * H * 4)))
+      (st = ensure(c, c->scratch, suppress_scratch_bytes(type, W, H))))
     return st;
   IPB_CUDA(cudaStreamWaitEvent(c->stream, c->last, 0), "cudaStreamWaitEvent");
   IPB_CUDA(cudaMemcpyAsync(c->img.p, image, bytes, cudaMemcpyHostToDevice, c->stream), "copy image");
-  IPB_CUDA(launch_suppress(type, c->img.p, W, H, radius, c->out.p, static_cast<uint32_t*>(c->scratch.p), c->stream),
+  IPB_CUDA(launch_suppress(type, c->img.p, W, H, radius, c->out.p, c->scratch.p, c->stream),
            "suppress_non_maximum launch");
   IPB_CUDA(cudaMemcpyAsync(out, c->out.p, bytes, cudaMemcpyDeviceToHost, c->stream), "copy output");
   return finish_sync(c, c->stream);
@@ -754,10 +754,10 @@ ipb_status device_suppress(int type, const void* d_image, uint32_t W, uint32_t H
   Context* c = nullptr;
   ipb_status st;
   if ((st = get_ctx(&c))) return st;
-  if ((st = ensure(c, c->scratch, (size_t)W * H * 4))) return st;
+  if ((st = ensure(c, c->scratch, suppress_scratch_bytes(type, W, H)))) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   IPB_CUDA(cudaStreamWaitEvent(s, c->last, 0), "cudaStreamWaitEvent");
-  IPB_CUDA(launch_suppress(type, d_image, W, H, radius, d_out, static_cast<uint32_t*>(c->scratch.p), s),
+  IPB_CUDA(launch_suppress(type, d_image, W, H, radius, d_out, c->scratch.p, s),
            "suppress_non_maximum launch");
   IPB_CUDA(cudaEventRecord(c->last, s), "cudaEventRecord");
   return IPB_OK;

@@ -94,8 +94,10 @@ cudaError_t launch_sat(const uint8_t* img, uint32_t W, uint32_t H, uint32_t chan
                        void* sat, cudaStream_t s);
 
 // ---- non-maximum suppression (tm_suppress.cu) -------------------------------
-// suppress_non_maximum of a W x H image of element `type` (ipb_elem_type); bx = W*H u32 scratch.
-cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
+// suppress_non_maximum of a W x H image of element `type` (ipb_elem_type);
+// scratch = suppress_scratch_bytes (each pixel's row-window winner: column and key).
+size_t suppress_scratch_bytes(int type, uint32_t W, uint32_t H);
+cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, void* scratch,
                             cudaStream_t s);
 size_t local_maxima_scratch_bytes(uint32_t n, uint32_t max_y);
 // local_maxima of n device points (max_y = the largest y): writes the kept

@@ -35,11 +35,19 @@
 namespace ipb {
 namespace {
 
+// Order-preserving key of a value: 32-bit for element types of 4 bytes or
+// less (halving the shared-memory scans), 64-bit otherwise.
 template <typename T>
-__device__ __forceinline__ unsigned long long okey(T v) {
+using KeyOf = typename std::conditional<(sizeof(T) <= 4), uint32_t, unsigned long long>::type;
+
+template <typename T>
+__device__ __forceinline__ KeyOf<T> okey(T v) {
   if constexpr (std::is_same<T, float>::value) {
     const uint32_t b = __float_as_uint(v);
-    return (b & 0x80000000u) ? (unsigned long long)(~b) : (unsigned long long)(b | 0x80000000u);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  } else if constexpr (sizeof(T) <= 4) {
+    if constexpr (std::is_signed<T>::value) return (uint32_t)(int32_t)v ^ 0x80000000u;
+    else return (uint32_t)v;
   } else if constexpr (std::is_signed<T>::value) {
     return (unsigned long long)(long long)v ^ 0x8000000000000000ull;
   } else {
@@ -48,35 +56,46 @@ __device__ __forceinline__ unsigned long long okey(T v) {
 }
 
 constexpr int kRowThreads = 256;
+constexpr int kRowBand = 8;  // rows per block of the row pass
 
-// Row pass: best column of the row window of every pixel, into `bx`.
+// Row pass: for every pixel, the column of its row window's winner (bx) and
+// that winner's key (bk). A block takes 256 columns (+ r halo) of kRowBand
+// rows, loads all their keys into shared memory at once, then scans.
 template <typename T>
 __global__ void __launch_bounds__(kRowThreads) snm_rows_kernel(const T* __restrict__ img, uint32_t W, uint32_t H,
-                                                               uint32_t r, uint32_t* __restrict__ bx) {
-  extern __shared__ unsigned long long s_key[];  // [kRowThreads + 2r] keys of the segment and its halo
+                                                               uint32_t r, uint32_t* __restrict__ bx,
+                                                               KeyOf<T>* __restrict__ bk) {
+  using K = KeyOf<T>;
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  K* s_key = reinterpret_cast<K*>(s_raw);  // [kRowBand][kRowThreads + 2r]
+  const uint32_t seg = kRowThreads + 2 * r;
   const uint32_t xs = blockIdx.x * kRowThreads;  // first pixel of the segment
   const uint32_t lo = xs > r ? xs - r : 0u;
   const uint32_t hi = (uint32_t)min((unsigned long long)W, (unsigned long long)xs + kRowThreads + r);
+  const uint32_t y0 = blockIdx.y * kRowBand;
+  const uint32_t nrow = min((uint32_t)kRowBand, H - y0);
+  for (uint32_t j = 0; j < nrow; ++j) {
+    const T* row = img + (size_t)(y0 + j) * W;
+    for (uint32_t c = lo + threadIdx.x; c < hi; c += kRowThreads) s_key[j * seg + c - lo] = okey(row[c]);
+  }
+  __syncthreads();
   const uint32_t x = xs + threadIdx.x;
-  for (uint32_t y = blockIdx.y; y < H; y += gridDim.y) {
-    const T* row = img + (size_t)y * W;
-    __syncthreads();  // the previous row's keys are no longer read
-    for (uint32_t c = lo + threadIdx.x; c < hi; c += kRowThreads) s_key[c - lo] = okey(row[c]);
-    __syncthreads();
-    if (x < W) {
-      const uint32_t a = x > r ? x - r : 0u;
-      const uint32_t b = (uint32_t)min((unsigned long long)W - 1, (unsigned long long)x + r);
-      uint32_t best = a;
-      unsigned long long bk = s_key[a - lo];
-      for (uint32_t c = a + 1; c <= b; ++c) {
-        const unsigned long long k = s_key[c - lo];
-        if (k > bk) {  // strictly greater: the smaller column wins among equals
-          bk = k;
-          best = c;
-        }
+  if (x >= W) return;
+  const uint32_t a = x > r ? x - r : 0u;
+  const uint32_t b = (uint32_t)min((unsigned long long)W - 1, (unsigned long long)x + r);
+  for (uint32_t j = 0; j < nrow; ++j) {
+    const K* kr = s_key + j * seg - lo;
+    uint32_t best = a;
+    K bkey = kr[a];
+    for (uint32_t c = a + 1; c <= b; ++c) {
+      const K k = kr[c];
+      if (k > bkey) {  // strictly greater: the smaller column wins among equals
+        bkey = k;
+        best = c;
       }
-      bx[(size_t)y * W + x] = best;
     }
+    bx[(size_t)(y0 + j) * W + x] = best;
+    bk[(size_t)(y0 + j) * W + x] = bkey;
   }
 }
 
@@ -85,7 +104,9 @@ __global__ void __launch_bounds__(kRowThreads) snm_rows_kernel(const T* __restri
 template <typename T>
 __global__ void __launch_bounds__(kRowThreads) snm_rows_global_kernel(const T* __restrict__ img, uint32_t W,
                                                                       uint32_t H, uint32_t r,
-                                                                      uint32_t* __restrict__ bx) {
+                                                                      uint32_t* __restrict__ bx,
+                                                                      KeyOf<T>* __restrict__ bk) {
+  using K = KeyOf<T>;
   const uint32_t x = blockIdx.x * kRowThreads + threadIdx.x;
   if (x >= W) return;
   for (uint32_t y = blockIdx.y; y < H; y += gridDim.y) {
@@ -93,15 +114,16 @@ __global__ void __launch_bounds__(kRowThreads) snm_rows_global_kernel(const T* _
     const uint32_t a = x > r ? x - r : 0u;
     const uint32_t b = (uint32_t)min((unsigned long long)W - 1, (unsigned long long)x + r);
     uint32_t best = a;
-    unsigned long long bk = okey(row[a]);
+    K bkey = okey(row[a]);
     for (uint32_t c = a + 1; c <= b; ++c) {
-      const unsigned long long k = okey(row[c]);
-      if (k > bk) {
-        bk = k;
+      const K k = okey(row[c]);
+      if (k > bkey) {
+        bkey = k;
         best = c;
       }
     }
     bx[(size_t)y * W + x] = best;
+    bk[(size_t)y * W + x] = bkey;
   }
 }
 
@@ -110,17 +132,19 @@ __global__ void __launch_bounds__(kRowThreads) snm_rows_global_kernel(const T* _
 // smaller y (the reference's tuple order (x, y)).
 template <typename T>
 __global__ void __launch_bounds__(256) snm_cols_kernel(const T* __restrict__ img, uint32_t W, uint32_t H, uint32_t r,
-                                                       const uint32_t* __restrict__ bx, T* __restrict__ out) {
+                                                       const uint32_t* __restrict__ bx,
+                                                       const KeyOf<T>* __restrict__ bk, T* __restrict__ out) {
+  using K = KeyOf<T>;
   const uint32_t x = blockIdx.x * 32 + (threadIdx.x & 31);
   const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (x >= W || y >= H) return;
   const uint32_t a = y > r ? y - r : 0u;
   const uint32_t b = (uint32_t)min((unsigned long long)H - 1, (unsigned long long)y + r);
   uint32_t wx = bx[(size_t)a * W + x], wy = a;
-  unsigned long long wk = okey(img[(size_t)a * W + wx]);
+  K wk = bk[(size_t)a * W + x];
   for (uint32_t yy = a + 1; yy <= b; ++yy) {
     const uint32_t cx = bx[(size_t)yy * W + x];
-    const unsigned long long k = okey(img[(size_t)yy * W + cx]);
+    const K k = bk[(size_t)yy * W + x];
     if (k > wk || (k == wk && cx < wx)) {  // equal x: the earlier row already holds
       wk = k;
       wx = cx;
@@ -132,18 +156,20 @@ __global__ void __launch_bounds__(256) snm_cols_kernel(const T* __restrict__ img
 }
 
 // Column pass through a shared-memory tile of 32 columns x 32 output rows and
-// r halo rows above and below: every row winner of the tile is gathered once
-// (its column and key, loads independent across the block), then each thread
-// scans its column window in shared memory.
+// r halo rows above and below: every row winner of the tile (its column and
+// key, both read coalesced) is staged once, then each thread scans its column
+// window in shared memory.
 constexpr int kColTile = 32;
 
 template <typename T>
 __global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict__ img, uint32_t W, uint32_t H,
                                                             uint32_t r, const uint32_t* __restrict__ bx,
-                                                            T* __restrict__ out) {
-  extern __shared__ unsigned long long s_wk[];  // [kColTile + 2r][32] winner keys, then [..][32] columns
+                                                            const KeyOf<T>* __restrict__ bk, T* __restrict__ out) {
+  using K = KeyOf<T>;
+  extern __shared__ __align__(16) unsigned char s_raw[];
   const uint32_t trows = kColTile + 2 * r;
-  uint32_t* s_wx = reinterpret_cast<uint32_t*>(s_wk + (size_t)trows * 32);
+  K* s_wk = reinterpret_cast<K*>(s_raw);                                    // [trows][32] winner keys
+  uint32_t* s_wx = reinterpret_cast<uint32_t*>(s_wk + (size_t)trows * 32);  // [trows][32] their columns
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t x = blockIdx.x * 32 + lane;
   const uint32_t y0 = blockIdx.y * kColTile;
@@ -151,9 +177,9 @@ __global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict_
   const uint32_t hi = (uint32_t)min((unsigned long long)H, (unsigned long long)y0 + kColTile + r);
   if (x < W)
     for (uint32_t i = warp; i < hi - lo; i += 8) {
-      const uint32_t yy = lo + i, cx = bx[(size_t)yy * W + x];
-      s_wx[i * 32 + lane] = cx;
-      s_wk[i * 32 + lane] = okey(img[(size_t)yy * W + cx]);
+      const size_t at = (size_t)(lo + i) * W + x;
+      s_wx[i * 32 + lane] = bx[at];
+      s_wk[i * 32 + lane] = bk[at];
     }
   __syncthreads();
   if (x >= W) return;
@@ -163,10 +189,10 @@ __global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict_
     const uint32_t a = y > r ? y - r : 0u;
     const uint32_t b = (uint32_t)min((unsigned long long)H - 1, (unsigned long long)y + r);
     uint32_t wx = s_wx[(a - lo) * 32 + lane], wy = a;
-    unsigned long long wk = s_wk[(a - lo) * 32 + lane];
+    K wk = s_wk[(a - lo) * 32 + lane];
     for (uint32_t yy = a + 1; yy <= b; ++yy) {
       const uint32_t cx = s_wx[(yy - lo) * 32 + lane];
-      const unsigned long long kk = s_wk[(yy - lo) * 32 + lane];
+      const K kk = s_wk[(yy - lo) * 32 + lane];
       if (kk > wk || (kk == wk && cx < wx)) {
         wk = kk;
         wx = cx;
@@ -178,29 +204,44 @@ __global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict_
 }
 
 template <typename T>
-cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, uint32_t* bx, cudaStream_t s) {
+cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, void* scratch, cudaStream_t s) {
+  using K = KeyOf<T>;
   if (W == 0 || H == 0) return cudaSuccess;
-  const dim3 rg((W + kRowThreads - 1) / kRowThreads, H < 65535u ? H : 65535u);
-  const size_t halo = (size_t)kRowThreads + 2 * (size_t)r;
-  if (halo * sizeof(unsigned long long) <= 48 * 1024)
-    snm_rows_kernel<T><<<rg, kRowThreads, halo * sizeof(unsigned long long), s>>>(img, W, H, r, bx);
-  else
-    snm_rows_global_kernel<T><<<rg, kRowThreads, 0, s>>>(img, W, H, r, bx);
+  uint32_t* bx = static_cast<uint32_t*>(scratch);
+  K* bk = reinterpret_cast<K*>(static_cast<uint8_t*>(scratch) + align_up((size_t)W * H * 4, 256));
+  const size_t band = (size_t)kRowBand * (kRowThreads + 2 * (size_t)r) * sizeof(K);
+  const uint32_t bands = (H + kRowBand - 1) / kRowBand;
+  if (band <= 48 * 1024 && bands <= 65535u) {
+    snm_rows_kernel<T><<<dim3((W + kRowThreads - 1) / kRowThreads, bands), kRowThreads, band, s>>>(img, W, H, r,
+                                                                                                   bx, bk);
+  } else {
+    const dim3 rg((W + kRowThreads - 1) / kRowThreads, H < 65535u ? H : 65535u);
+    snm_rows_global_kernel<T><<<rg, kRowThreads, 0, s>>>(img, W, H, r, bx, bk);
+  }
   count_launch(kKernelSuppress);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const size_t tile_bytes = ((size_t)kColTile + 2 * (size_t)r) * 32 * 12;
+  const size_t tile_bytes = ((size_t)kColTile + 2 * (size_t)r) * 32 * (sizeof(K) + 4);
   if (tile_bytes <= 48 * 1024) {
     if ((H + kColTile - 1) / kColTile > 65535u) return cudaErrorInvalidValue;  // images up to 2097120 rows
     snm_cols_tile_kernel<T><<<dim3((W + 31) / 32, (H + kColTile - 1) / kColTile), 256, tile_bytes, s>>>(
-        img, W, H, r, bx, out);
+        img, W, H, r, bx, bk, out);
   } else {
     if ((H + 7) / 8 > 65535u) return cudaErrorInvalidValue;  // images up to 524280 rows
-    snm_cols_kernel<T><<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, s>>>(img, W, H, r, bx, out);
+    snm_cols_kernel<T><<<dim3((W + 31) / 32, (H + 7) / 8), 256, 0, s>>>(img, W, H, r, bx, bk, out);
   }
   count_launch(kKernelSuppress);
   return cudaGetLastError();
 }
+
+}  // namespace
+
+size_t suppress_scratch_bytes(int type, uint32_t W, uint32_t H) {
+  const size_t key = (type == IPB_ELEM_U64 || type == IPB_ELEM_I64) ? 8 : 4;
+  return align_up((size_t)W * H * 4, 256) + (size_t)W * H * key;
+}
+
+namespace {
 
 // ---- local_maxima ------------------------------------------------------------
 
@@ -266,7 +307,7 @@ __global__ void lm_compact_kernel(const uint32_t* flags, const uint32_t* pos, co
 
 }  // namespace
 
-cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, uint32_t* bx,
+cudaError_t launch_suppress(int type, const void* img, uint32_t W, uint32_t H, uint32_t r, void* out, void* bx,
                             cudaStream_t s) {
   switch (type) {
     case IPB_ELEM_U8: return launch_snm_t(static_cast<const uint8_t*>(img), W, H, r, static_cast<uint8_t*>(out), bx, s);
