@@ -50,7 +50,7 @@ void settle_pending_locked() {
     if (cudaEventSynchronize(t.timer.end) == cudaSuccess &&
         cudaEventElapsedTime(&ms, t.timer.begin, t.timer.end) == cudaSuccess && t.timer.kernel >= 0) {
       KernelStats& k = g_stats[t.timer.kernel];
-      k.launches += 1;
+      k.launches += t.timer.launches;
       k.ms += ms;
       k.macs += t.macs;
       k.bytes += t.bytes;
@@ -72,6 +72,7 @@ KernelTimer* acquire_timer() {
     return nullptr;
   }
   t.kernel = -1;
+  t.launches = 1;
   g_pending.push_back({t, 0.0, 0.0});
   return &g_pending.back().timer;
 }

@@ -11,6 +11,10 @@
 //   * tensor-core pairs are grouped by tensor-memory row width and mask
 //     kind, and each group runs as ONE persistent launch over all its tiles
 //     with find_extremes fused into the epilogue;
+//   * the groups' launches run side by side on two streams, the group with
+//     the longest tiles first, each claiming tiles from its own counter, so
+//     the SMs that one launch leaves idle in its last wave take tiles of the
+//     next instead of waiting for the slowest CTA;
 //   * the launch sequence is captured once in a CUDA graph and replayed.
 #include <algorithm>
 #include <chrono>
@@ -55,6 +59,11 @@ struct ipb_batch_plan {
   ipb::ExtremesResult<float>* d_ext_result = nullptr;
   unsigned int* d_err = nullptr;
   unsigned int tag = 0;
+  // tile counters of the groups' launches (two words each) and, with two or
+  // more groups, the stream and events the later groups run on
+  unsigned int* d_sched = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint32_t kernels = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -162,8 +171,11 @@ void release(ipb_batch_plan* p) {
   for (auto& g : p->groups)
     if (g.d_probs) cudaFree(g.d_probs);
   for (void* b : {(void*)p->d_keys, (void*)p->d_widths, (void*)p->d_outs, p->d_scratch, p->d_ext_scratch,
-                  (void*)p->d_ext_result, (void*)p->d_err})
+                  (void*)p->d_ext_result, (void*)p->d_err, (void*)p->d_sched})
     if (b) cudaFree(b);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
+  if (p->side) cudaStreamDestroy(p->side);
 }
 
 // Enqueue the plan's launch sequence (used once under stream capture, and
@@ -174,7 +186,22 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     IPB_TRY(launch_extremes_keys_init(p->d_keys, p->nkeys, s), "extremes init");
     ++k;
   }
-  for (auto& g : p->groups) {
+  // groups after the first run on the side stream, between a fork and a join
+  // on s; concurrent launches are timed as one span on s
+  const bool side_by_side = p->groups.size() >= 2 && p->side;
+  KernelTimer* span = timed && side_by_side ? acquire_kernel_timer() : nullptr;
+  double span_macs = 0, span_bytes = 0;
+  if (span) {
+    timer_begin(span, kKernelUmma, s);
+    span->launches = (uint32_t)p->groups.size();
+  }
+  if (side_by_side) {
+    IPB_TRY(cudaEventRecord(p->ev_fork, s), "fork");
+    IPB_TRY(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "fork");
+  }
+  for (size_t gi = 0; gi < p->groups.size(); ++gi) {
+    const ipb_batch_plan::Group& g = p->groups[gi];
+    const cudaStream_t gs = side_by_side && gi > 0 ? p->side : s;
     UmmaLaunch L{};
     const uint32_t n = (uint32_t)g.probs.size();
     if (n <= kInlineProblems)
@@ -184,19 +211,28 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     L.tiles = g.tiles;
     L.err = p->d_err;
     L.tag = p->tag;
-    KernelTimer* t = timed ? acquire_kernel_timer() : nullptr;
-    IPB_TRY(launch_umma_batch(g.plan, L, s, t), "tensor-core batch launch");
-    if (t) {
-      double macs = 0, bytes = 0;
-      for (uint32_t i : g.members) {
-        const MatchArgs& a = p->args[i];
-        const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
-        macs += Wo * Ho * tp;
-        bytes += (double)a.W * a.H + tp * (a.mask ? 2.0 : 1.0) + 4.0 * Wo * Ho;
-      }
-      note_kernel_timed(t, macs, bytes);
+    L.sched = p->d_sched + 2 * gi;
+    KernelTimer* t = timed && !side_by_side ? acquire_kernel_timer() : nullptr;
+    IPB_TRY(launch_umma_batch(g.plan, L, gs, t), "tensor-core batch launch");
+    double macs = 0, bytes = 0;
+    for (uint32_t i : g.members) {
+      const MatchArgs& a = p->args[i];
+      const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
+      macs += Wo * Ho * tp;
+      bytes += (double)a.W * a.H + tp * (a.mask ? 2.0 : 1.0) + 4.0 * Wo * Ho;
     }
+    if (t) note_kernel_timed(t, macs, bytes);
+    span_macs += macs;
+    span_bytes += bytes;
     ++k;
+  }
+  if (side_by_side) {
+    IPB_TRY(cudaEventRecord(p->ev_join, p->side), "join");
+    IPB_TRY(cudaStreamWaitEvent(s, p->ev_join, 0), "join");
+  }
+  if (span) {
+    timer_end(span, s);
+    note_kernel_timed(span, span_macs, span_bytes);
   }
   for (size_t i = 0; i < p->args.size(); ++i) {
     if (p->tensor[i]) continue;
@@ -329,6 +365,24 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
       cudaMemcpy(g.d_probs, g.probs.data(), sizeof(UmmaProblem) * g.probs.size(), cudaMemcpyHostToDevice);
     }
     p->groups.push_back(std::move(g));
+  }
+  // longest tiles first (binary masks: three correlations per row; then the
+  // widest rows), so that the launch started second fills the tail of the first
+  std::stable_sort(p->groups.begin(), p->groups.end(),
+                   [](const ipb_batch_plan::Group& x, const ipb_batch_plan::Group& y) {
+                     if (x.plan.masked != y.plan.masked) return x.plan.masked;
+                     return x.plan.ks > y.plan.ks;
+                   });
+  if (!p->groups.empty()) {
+    const size_t sched_bytes = sizeof(unsigned int) * 2 * p->groups.size();
+    if ((e = cudaMalloc(&p->d_sched, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMalloc"));
+    if ((e = cudaMemset(p->d_sched, 0, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
+  }
+  if (p->groups.size() >= 2) {
+    if ((e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess)
+      return fail(to_status(e, "side stream"));
   }
   if ((e = umma_prepare_kernels()) != cudaSuccess) return fail(to_status(e, "kernel attributes"));
   uint32_t kernels = 0;

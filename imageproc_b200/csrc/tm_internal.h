@@ -34,6 +34,7 @@ struct KernelTimer {
   cudaEvent_t begin = nullptr;
   cudaEvent_t end = nullptr;
   int kernel = -1;  // set by the launcher: which kernel was timed
+  uint32_t launches = 1;  // launches inside the span (concurrent launches timed together)
 };
 
 // One (image, template[, mask]) matching problem, all pointers on the device.
@@ -161,6 +162,10 @@ struct UmmaLaunch {
   uint32_t z_off, img_off, rs_off;
   unsigned int* err;
   unsigned int tag;
+  // {next tile counter, CTAs finished}, both zero at launch: tiles after the
+  // first wave are claimed from it; the last CTA out zeroes it again.
+  // Null: a fixed grid stride.
+  unsigned int* sched;
 };
 
 // Launch-wide plan of a group of problems sharing (tensor-memory row width,

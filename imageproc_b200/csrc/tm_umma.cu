@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   uint64_t* drain = dfull + 1;
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + 128);
   volatile int* s_err = reinterpret_cast<volatile int*>(smem + 132);
+  volatile uint32_t* s_next = reinterpret_cast<volatile uint32_t*>(smem + 136);  // tile after the current one
   unsigned long long* s_part = reinterpret_cast<unsigned long long*>(smem + 256);  // kWarps partial sums
   uint8_t* zbuf = smem + L.z_off;
   uint8_t* s_img = smem + L.img_off;
@@ -324,9 +325,13 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   uint32_t tss = 0;
   bool ok = true;
 
-  for (uint32_t tile = blockIdx.x; tile < L.tiles; tile += gridDim.x, ++tcount) {
+  for (uint32_t tile = blockIdx.x, next = 0; tile < L.tiles; tile = next, ++tcount) {
     __syncthreads();
     if (*s_err) break;
+    // the tile after this one: drawn from the launch's counter when it
+    // schedules dynamically (a CTA that starts late, behind another launch,
+    // takes fewer tiles), else a fixed grid stride. Claims rise monotonically.
+    if (threadIdx.x == 0) *s_next = L.sched ? gridDim.x + atomicAdd(L.sched, 1u) : tile + gridDim.x;
     pi = find_problem(L, P, pi, tile);
     // a register copy: the tcgen05/cp.async asm statements clobber memory,
     // which would otherwise force every use to reload the field
@@ -394,6 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     cp_async_wait_all();
     __syncthreads();
     if (*s_err) break;
+    next = *s_next;
     if (new_z) {
       unsigned long long t = 0;
       for (int k = 0; k < kWarps; ++k) t += s_part[k];
@@ -426,9 +432,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       __syncthreads();
     }
     // the next tile's rows stream into the other buffer during this tile
-    if (L.nbuf == 2 && tile + gridDim.x < L.tiles) {
-      const uint32_t pn = find_problem(L, P, pi, tile + gridDim.x);
-      issue_tile_load(L, P[pn], s_img + (buf ^ 1u) * NPL * L.plane_bytes, tile + gridDim.x - P[pn].tile_begin);
+    if (L.nbuf == 2 && next < L.tiles) {
+      const uint32_t pn = find_problem(L, P, pi, next);
+      issue_tile_load(L, P[pn], s_img + (buf ^ 1u) * NPL * L.plane_bytes, next - P[pn].tile_begin);
     }
     const uint32_t nst = (nrows + L.rps - 1) / L.rps;
     const unsigned long long deadline = global_ns() + kWaitNs;
@@ -552,6 +558,15 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   // drain outstanding copies and MMAs, then free tensor memory
   cp_async_wait_all();
   __syncthreads();
+  if (L.sched && threadIdx.x == 0) {
+    // every CTA has made its last claim before it counts itself out, so the
+    // last one out re-arms the counter for the next launch that uses it
+    __threadfence();
+    if (atomicAdd(L.sched + 1, 1u) == gridDim.x - 1) {
+      atomicExch(L.sched, 0u);
+      atomicExch(L.sched + 1, 0u);
+    }
+  }
   if (mma_warp) {
     mma_commit_warp(drain);
     if (!mbar_wait(drain, 0, global_ns() + kWaitNs) && lane == 0) atomicMax(L.err, L.tag);

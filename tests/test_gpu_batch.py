@@ -94,6 +94,42 @@ def test_batch_plan_graph_replay():
     plan.close()
 
 
+def test_batch_groups_side_by_side_claim_every_tile_once():
+    # an unmasked and a binary-mask group, each with more tiles than SMs, so
+    # CTAs claim tiles from the launch's counter while the two launches run on
+    # two streams; run four times (a one-off plan, the plan's graph, the plan
+    # enqueued directly with its kernels timed, the graph again) over NaN-filled
+    # outputs, so a tile skipped or a counter left armed shows as a mismatch
+    import torch
+
+    from imageproc_b200 import device
+    g = np.random.default_rng(11)
+    image = g.integers(0, 256, (640, 1024), dtype=np.uint8)
+    template = g.integers(0, 256, (40, 48), dtype=np.uint8)
+    mask = (g.random((40, 48)) < 0.8).astype(np.uint8)
+    items = [(image, template, m, None) for m in range(4)] + [(image, template, m, mask) for m in range(4)]
+    batch = device.Batch(_to_device(items))
+    plan = device.BatchPlan(batch)
+    assert plan.info()["tensor_pairs"] == 8
+    expected = [O.match_exact(image, template, m, mk, precision=0) for image, template, m, mk in items]
+    _lib.profile_collect()  # drop stats left by earlier calls
+    for launch, timed in ((batch.run, False), (plan.launch, False), (plan.launch, True), (plan.launch, False)):
+        for o in batch.outs:
+            o.fill_(float("nan"))
+        batch.extremes.zero_()
+        _lib.profile_enable(timed)  # timed: the plan's launches enqueued directly, not as its graph
+        try:
+            launch()
+            torch.cuda.synchronize()
+        finally:
+            _lib.profile_enable(False)
+        for k, (out, exp) in enumerate(zip(batch.outs, expected)):
+            bad = np.argwhere(bits(out.cpu().numpy()) != bits(exp))
+            assert bad.size == 0, (k, timed, bad[:3])
+    assert _lib.profile_collect()["umma_i8"]["launches"] == 2  # the two side-by-side launches, timed as one span
+    plan.close()
+
+
 def test_batch_of_more_problems_than_fit_in_kernel_parameters():
     # > 8 tensor pairs of one group: problem descriptors come from device memory
     from imageproc_b200 import device
