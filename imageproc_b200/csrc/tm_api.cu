@@ -173,8 +173,10 @@ struct Context {
   unsigned int tag = 0;            // tag of the last tensor-core launch
   unsigned int tag_checked = 0;    // largest failing tag already reported
   bool tensor_since_check = false;
-  // copy streams of the banded host calls: image rows in, score rows out
+  // copy streams of the banded host calls: image rows in, score rows out;
+  // tensor-core bands run on streams of their own
   cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaStream_t s_band[kMaxBands] = {};
   cudaEvent_t band_in[kMaxBands] = {}, band_done[kMaxBands] = {}, out_done = nullptr;
   ~Context() {
     if (device < 0) return;
@@ -183,6 +185,10 @@ struct Context {
     for (cudaStream_t s : {s_in, s_out})
       if (s) cudaStreamSynchronize(s);
     for (uint32_t b = 0; b < kMaxBands; ++b) {
+      if (s_band[b]) {
+        cudaStreamSynchronize(s_band[b]);
+        cudaStreamDestroy(s_band[b]);
+      }
       if (band_in[b]) cudaEventDestroy(band_in[b]);
       if (band_done[b]) cudaEventDestroy(band_done[b]);
     }
@@ -331,9 +337,11 @@ uint32_t host_bands(size_t out_bytes, uint32_t Ho, uint32_t w, uint32_t h) {
   return std::min(n, (Ho + 15) / 16);  // bands of at least 16 score rows
 }
 
-ipb_status ensure_band_streams(Context* c) {
+ipb_status ensure_band_streams(Context* c, uint32_t nb) {
   for (cudaStream_t* s : {&c->s_in, &c->s_out})
     if (!*s) IPB_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (uint32_t b = 0; b < nb; ++b)
+    if (!c->s_band[b]) IPB_CUDA(cudaStreamCreateWithFlags(&c->s_band[b], cudaStreamNonBlocking), "cudaStreamCreate");
   for (uint32_t b = 0; b < kMaxBands; ++b) {
     if (!c->band_in[b]) IPB_CUDA(cudaEventCreateWithFlags(&c->band_in[b], cudaEventDisableTiming), "cudaEventCreate");
     if (!c->band_done[b])
@@ -348,15 +356,40 @@ ipb_status ensure_band_streams(Context* c) {
 // rows keep the full map's pitch, so every score is the one the whole-map
 // launch writes. Image rows cross once, in order (a band copies only the rows
 // the previous band did not); bands start on multiples of 16 rows so a
-// 16-byte-aligned image stays aligned.
+// 16-byte-aligned image stays aligned. A band is under one wave of SMs, so
+// a launch of it takes about as long as the whole map's: tensor-core bands
+// therefore run on streams of their own, each starting once its image rows
+// are in, beside the bands before it (they share no scratch). CUDA-core bands
+// share the context's scratch and run in order on the context's stream.
 ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* image, const uint8_t* tpl,
                              const uint8_t* mask, uint32_t nb, float* out) {
   ipb_status st;
-  if ((st = ensure_band_streams(c))) return st;
+  if ((st = ensure_band_streams(c, nb))) return st;
+  const bool side_by_side =
+      full.precision != IPB_PRECISION_REFERENCE_F32 && g_path.load() != 1 && umma_supported(full);
+  if (side_by_side && (st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
+  // A copy into page-locked memory returns at once, so a band's score rows are
+  // queued as soon as its launch is: they cross while the host still copies
+  // later image rows from pageable memory (which holds the calling thread).
+  // Into pageable memory the copy would hold the thread too: queued last.
+  cudaPointerAttributes pa{};
+  bool out_locked = false;
+  if (cudaPointerGetAttributes(&pa, out) == cudaSuccess)
+    out_locked = pa.type == cudaMemoryTypeHost;
+  else
+    (void)cudaGetLastError();  // not a pointer the runtime knows: pageable
   const uint32_t W = full.W, Wo = full.W - full.w + 1, Ho = full.H - full.h + 1;
   const size_t tb = (size_t)full.w * full.h;
   const uint32_t rows = (uint32_t)align_up((Ho + nb - 1) / nb, 16);
   uint8_t* d_img = static_cast<uint8_t*>(c->img.p);
+  auto queue_out = [&](uint32_t b) -> ipb_status {
+    const uint32_t o0 = b * rows, o1 = std::min(Ho, o0 + rows);
+    IPB_CUDA(cudaStreamWaitEvent(c->s_out, c->band_done[b], 0), "cudaStreamWaitEvent");
+    IPB_CUDA(cudaMemcpyAsync(out + (size_t)o0 * Wo, full.out + (size_t)o0 * Wo, (size_t)(o1 - o0) * Wo * sizeof(float),
+                             cudaMemcpyDeviceToHost, c->s_out),
+             "copy score rows");
+    return IPB_OK;
+  };
   auto enqueue = [&]() -> ipb_status {
     IPB_CUDA(cudaStreamWaitEvent(c->s_in, c->last, 0), "cudaStreamWaitEvent");
     IPB_CUDA(cudaMemcpyAsync(c->tpl.p, tpl, tb, cudaMemcpyHostToDevice, c->s_in), "copy template");
@@ -369,23 +402,33 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
                "copy image rows");
       have = need;
       IPB_CUDA(cudaEventRecord(c->band_in[bands], c->s_in), "cudaEventRecord");
-      IPB_CUDA(cudaStreamWaitEvent(c->stream, c->band_in[bands], 0), "cudaStreamWaitEvent");
       MatchArgs a = full;
       a.img = full.img + (size_t)o0 * W;
       a.H = need - o0;
       a.out = full.out + (size_t)o0 * Wo;
-      ipb_status s2 = run_match(c, a);
-      if (s2) return s2;
-      IPB_CUDA(cudaEventRecord(c->band_done[bands], c->stream), "cudaEventRecord");
+      if (side_by_side) {
+        a.stream = c->s_band[bands];
+        IPB_CUDA(cudaStreamWaitEvent(a.stream, c->band_in[bands], 0), "cudaStreamWaitEvent");
+        a.timer = acquire_timer();
+        c->tag += 1;
+        c->tensor_since_check = true;
+        const cudaError_t e = launch_umma(a, static_cast<unsigned int*>(c->errw.p), c->tag);
+        if (a.timer) {
+          const double tp = (double)a.w * a.h, Ho_b = a.H - a.h + 1.0;
+          note_timed(a.timer, Wo * Ho_b * tp, (double)a.W * a.H + tp * (a.mask ? 2.0 : 1.0) + 4.0 * Wo * Ho_b);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "template-matching launch");
+      } else {
+        IPB_CUDA(cudaStreamWaitEvent(c->stream, c->band_in[bands], 0), "cudaStreamWaitEvent");
+        ipb_status s2 = run_match(c, a);
+        if (s2) return s2;
+      }
+      IPB_CUDA(cudaEventRecord(c->band_done[bands], a.stream), "cudaEventRecord");
+      if (out_locked && (st = queue_out(bands))) return st;
     }
-    // queued after every launch: a copy to pageable memory blocks the host
-    for (uint32_t b = 0; b < bands; ++b) {
-      const uint32_t o0 = b * rows, o1 = std::min(Ho, o0 + rows);
-      IPB_CUDA(cudaStreamWaitEvent(c->s_out, c->band_done[b], 0), "cudaStreamWaitEvent");
-      IPB_CUDA(cudaMemcpyAsync(out + (size_t)o0 * Wo, full.out + (size_t)o0 * Wo, (size_t)(o1 - o0) * Wo * sizeof(float),
-                               cudaMemcpyDeviceToHost, c->s_out),
-               "copy score rows");
-    }
+    if (!out_locked)
+      for (uint32_t b = 0; b < bands; ++b)
+        if ((st = queue_out(b))) return st;
     IPB_CUDA(cudaEventRecord(c->out_done, c->s_out), "cudaEventRecord");
     IPB_CUDA(cudaStreamWaitEvent(c->stream, c->out_done, 0), "cudaStreamWaitEvent");
     return IPB_OK;
@@ -394,6 +437,7 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
     // nothing may touch the caller's buffers after the call returns
     cudaStreamSynchronize(c->s_in);
     cudaStreamSynchronize(c->stream);
+    for (uint32_t b = 0; b < nb; ++b) cudaStreamSynchronize(c->s_band[b]);
     cudaStreamSynchronize(c->s_out);
     return st;
   }
