@@ -523,27 +523,36 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         tc_fence_after();
         const uint32_t r0 = st * L.rps, cnt = min(nrows, r0 + L.rps) - r0;
         const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
-#pragma unroll 4
-        for (uint32_t i = 0; i < kMaxRps; ++i) {
-          if (i >= cnt) break;
-          const uint4 bd = band[r0 + i];  // n0, idesc, first Z row of the band
-          const uint32_t n0 = bd.x, idesc = bd.y;
-          const uint32_t zrow = dlo + bd.z;
-          const uint32_t a = a_stage + i * a_row_cols;
-          if (leader) {
+        if (leader) {
+          // the elected lane alone walks the stage's rows, reading four band
+          // entries {n0, idesc, first Z row} ahead of their MMAs. The reads
+          // run at most three entries past the tile's last row: still inside
+          // shared memory (the Z buffers follow the table), and unused.
+          for (uint32_t i0 = 0; i0 < cnt; i0 += 4) {
+            uint4 bd[4];
 #pragma unroll
-            for (int c = 0; c < NCORR; ++c) {
-              const uint32_t zo = zrow + (c == 0 ? 0u : zoff1);
+            for (int j = 0; j < 4; ++j) bd[j] = band[r0 + i0 + j];
 #pragma unroll
-              for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
-                if (kk < ksteps)
-                  mma_i8_ts(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
-                            ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
+            for (int j = 0; j < 4; ++j) {
+              if (i0 + j < cnt) {
+                const uint32_t n0 = bd[j].x, idesc = bd[j].y;
+                const uint32_t zrow = dlo + bd[j].z;
+                const uint32_t a = a_stage + (i0 + j) * a_row_cols;
+#pragma unroll
+                for (int c = 0; c < NCORR; ++c) {
+                  const uint32_t zo = zrow + (c == 0 ? 0u : zoff1);
+#pragma unroll
+                  for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
+                    if (kk < ksteps)
+                      mma_i8_ts(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                                ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
+                  }
+                }
               }
             }
           }
+          mma_commit(&empty[s]);
         }
-        if (leader) mma_commit(&empty[s]);
         __syncwarp();
       }
       if (ok && leader) mma_commit(dfull);
