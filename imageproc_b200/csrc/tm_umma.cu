@@ -10,15 +10,20 @@
 // Formulation. A CTA owns a tile of 128 output columns (x0 + m, m = tensor-
 // memory lane) by NT output rows (y0 + n, n = tensor-memory column). For each
 // image row r of the tile (r = 0 .. NT + h - 2, image row y0 + r) and each
-// correlation c:
+// correlation c, into accumulator a(c):
 //   A_r[m][k] = P_c[y0 + r][x0 + m + k]          (a Hankel row per lane)
 //   B_r[n][k] = Q_c[r - n][k]                     (0 <= r - n < h, else 0)
-//   D_c[m][n] += sum_k A_r[m][k] * B_r[n][k]
-// so that after all rows D_c[m][n] = sum_{dy,dx} P_c[y0+n+dy][x0+m+dx] Q_c[dy][dx].
-//   unmasked:     c = 0: P = I, Q = T                          -> X
-//   binary mask:  c = 0: P = I, Q = T*m                        -> X
-//                 c = 1: P = low byte of I^2,  Q = m           \ Y = D_1 + 256 D_2
-//                 c = 2: P = high byte of I^2, Q = m           /
+//   D_a(c)[m][n] += sum_k A_r[m][k] * B_r[n][k]
+// so that after all rows D_a[m][n] = sum over c with a(c) = a of
+// sum_{dy,dx} P_c[y0+n+dy][x0+m+dx] Q_c[dy][dx].
+//   unmasked:     c = 0: P = I, Q = T,                      a = 0  -> X
+//   binary mask:  c = 0: P = I, Q = T*m,                    a = 0  -> X
+//                 c = 1: P = I^2 mod 255,       Q = m,      a = 1  \ Y
+//                 c = 2: P = floor(I^2 / 255),  Q = 255*m,  a = 1  /
+// Both parts of I^2 = 255 floor(I^2/255) + I^2 mod 255 lie in 0..255, and
+// 255*m is a u8 for a binary mask, so the two u8 x u8 correlations sum to
+// Y = sum I^2 m in one accumulator, exactly: every partial sum is at most
+// 65025 * 16384 < 2^31 for the masked template sizes taken here.
 // B_r is a window of one buffer Z_c (Q_c with its rows reversed and 16 zero
 // rows on each side) stored in the canonical no-swizzle K-major layout, whose
 // rows are 16 bytes apart: moving from r to r+1 moves B's start address by
@@ -189,11 +194,9 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
   for (uint32_t n0 = e.c_begin; n0 < e.c_begin + e.ncols; n0 += 16) {
     uint32_t vx[16];
     tmem_ld16(tmem_addr(e.tmem, e.lane_base, n0), vx);
-    uint32_t vl[MASKED ? 16 : 1], vh[MASKED ? 16 : 1];
     uint32_t yv[16];
     if constexpr (MASKED) {
-      tmem_ld16(tmem_addr(e.tmem, e.lane_base, e.NT + n0), vl);
-      tmem_ld16(tmem_addr(e.tmem, e.lane_base, 2 * e.NT + n0), vh);
+      tmem_ld16(tmem_addr(e.tmem, e.lane_base, e.NT + n0), yv);
     } else {
       // window sums of the chunk: loads first, then the sliding chain
       uint32_t add[16], subv[16];
@@ -214,11 +217,8 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       const uint32_t y = e.y0 + n0 + k;
-      uint32_t Yk;
-      if constexpr (MASKED) Yk = vl[k] + (vh[k] << 8);
-      else Yk = yv[k];
       if (e.x < q.Wo && y < q.Ho) {
-        const float f = finish_score32(kMethod, kPrec, vx[k], Yk, e.tss);
+        const float f = finish_score32(kMethod, kPrec, vx[k], yv[k], e.tss);
         const uint32_t lin = y * q.Wo + e.x;
         q.out[(size_t)lin] = f;
         if constexpr (kExt) {
@@ -267,9 +267,10 @@ __device__ __forceinline__ void umma_epilogue_dispatch(const UmmaEpi& e, int met
 
 template <int KS, bool MASKED>
 __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_constant__ UmmaLaunch L) {
-  constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, low, high byte of I^2)
-  constexpr int NCORR = MASKED ? 3 : 1;  // correlations / accumulators
-  constexpr int NZ = MASKED ? 2 : 1;     // reversed-template buffers
+  constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, I^2 mod 255, floor(I^2 / 255))
+  constexpr int NCORR = MASKED ? 3 : 1;  // correlations, one per plane
+  constexpr int NACC = MASKED ? 2 : 1;   // accumulators: X (, Y)
+  constexpr int NZ = MASKED ? 3 : 1;     // reversed-template buffers, one per correlation
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kStages;
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  const uint32_t a_col0 = NCORR * L.NT;
+  const uint32_t a_col0 = NACC * L.NT;
   const uint32_t a_row_cols = NPL * KS;
 
   uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     if (new_z) {
       // Z buffers, K-chunk-major: chunk c holds rows j = 0..zrows-1 of 16 bytes,
       // row j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
-      //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m
+      //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m, Z_2 from 255*m
       const uint32_t nchunks = q.kmma / 16;
       for (uint32_t idx = threadIdx.x; idx < NZ * nchunks * q.zrows; idx += kThreads) {
         const uint32_t zp = idx / (nchunks * q.zrows);
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
               uint32_t v;
               if constexpr (MASKED) {
                 const uint32_t mv = __ldg(q.mask + row + dx);
-                v = zp == 0 ? (uint32_t)__ldg(q.tpl + row + dx) * mv : mv;
+                v = zp == 0 ? (uint32_t)__ldg(q.tpl + row + dx) * mv : (zp == 1 ? mv : 255u * mv);
               } else {
                 v = __ldg(q.tpl + row + dx);
               }
@@ -411,23 +412,25 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       z_kmma = q.kmma;
     }
     if constexpr (MASKED) {
-      // byte planes of I^2 next to the staged image
+      // the two u8 parts of I^2 (I^2 mod 255, floor(I^2 / 255)) next to the
+      // staged image
       const uint32_t words = nrows * L.imgp / 4;
       const uint32_t* i4 = reinterpret_cast<const uint32_t*>(img_buf);
-      uint32_t* lo4 = reinterpret_cast<uint32_t*>(img_buf + L.plane_bytes);
-      uint32_t* hi4 = reinterpret_cast<uint32_t*>(img_buf + 2 * L.plane_bytes);
+      uint32_t* rem4 = reinterpret_cast<uint32_t*>(img_buf + L.plane_bytes);
+      uint32_t* quo4 = reinterpret_cast<uint32_t*>(img_buf + 2 * L.plane_bytes);
       for (uint32_t idx = threadIdx.x; idx < words; idx += kThreads) {
         const uint32_t v = i4[idx];
-        uint32_t lo = 0, hi = 0;
+        uint32_t rem = 0, quo = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const uint32_t b = (v >> (8 * k)) & 0xFFu;
           const uint32_t sq = b * b;
-          lo |= (sq & 0xFFu) << (8 * k);
-          hi |= (sq >> 8) << (8 * k);
+          const uint32_t qd = sq / 255u;  // 0..255
+          rem |= (sq - 255u * qd) << (8 * k);
+          quo |= qd << (8 * k);
         }
-        lo4[idx] = lo;
-        hi4[idx] = hi;
+        rem4[idx] = rem;
+        quo4[idx] = quo;
       }
       __syncthreads();
     }
@@ -449,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       {
         const uint32_t zero16[16] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
-        for (int c = 0; c < NCORR; ++c)
+        for (int c = 0; c < NACC; ++c)
           for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
             tmem_st16(tmem_addr(tmem, lane_base, c * L.NT + col), zero16);
       }
@@ -540,11 +543,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
                 const uint32_t a = a_stage + (i0 + j) * a_row_cols;
 #pragma unroll
                 for (int c = 0; c < NCORR; ++c) {
-                  const uint32_t zo = zrow + (c == 0 ? 0u : zoff1);
+                  const uint32_t zo = zrow + c * zoff1;
+                  const uint32_t acc = c == 0 ? 0u : 1u;  // X, or Y for both parts of I^2
 #pragma unroll
                   for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
                     if (kk < ksteps)
-                      mma_i8_ts(tmem + c * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                      mma_i8_ts(tmem + acc * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
                                 ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
                   }
                 }
@@ -625,7 +629,7 @@ uint32_t ks_of(uint32_t w) {
 // Kernel-wide tile and shared-memory plan for a group sharing (ks, masked):
 // sized for the group's tallest template.
 bool make_plan(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
-  const uint32_t npl = masked ? 3 : 1, ncorr = masked ? 3 : 1, nz = masked ? 2 : 1;
+  const uint32_t npl = masked ? 3 : 1, nacc = masked ? 2 : 1, nz = masked ? 3 : 1;
   pl.ks = ks;
   pl.masked = masked;
   pl.imgp = kM + 4 * ks + 16;
@@ -633,7 +637,7 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
   const uint32_t zplane = (kmma / 16) * (hmax + 32) * 16;
   const uint32_t nts[2] = {masked ? 64u : 128u, 64u};
   for (uint32_t nt : nts) {
-    const uint32_t tm_left = kTmemCols - ncorr * nt;
+    const uint32_t tm_left = kTmemCols - nacc * nt;
     const uint32_t rps = tm_left / (kStages * npl * ks);
     if (rps < 1) continue;
     const uint32_t rows = nt + hmax - 1;
