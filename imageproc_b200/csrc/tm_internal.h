@@ -179,6 +179,7 @@ struct UmmaPlan {
 uint32_t umma_group_key(const MatchArgs& a);
 // Sets every tensor-core kernel's shared-memory limit (outside stream capture).
 cudaError_t umma_prepare_kernels();
+// Plan of a batch group (launches of many tiles: the tallest tiles that fit).
 bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl);
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
                          unsigned long long* ext_keys);

@@ -447,8 +447,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t q4 = warp & 3, sub = warp >> 2;
       const uint32_t m = q4 * 32 + lane;
       const uint32_t lane_base = q4 * 32;
-      const uint32_t ncols = L.NT / kSubs;  // accumulator columns this warp zeroes and finishes
-      const uint32_t c_begin = sub * ncols;
+      // accumulator columns this warp zeroes and finishes: the tile's 16-column
+      // chunks shared out over the quadrant's kSubs warps (unevenly when NT / 16
+      // is not a multiple of kSubs)
+      const uint32_t chunks = L.NT / 16;
+      const uint32_t c_begin = 16 * (sub * chunks / kSubs);
+      const uint32_t ncols = 16 * ((sub + 1) * chunks / kSubs) - c_begin;
       {
         const uint32_t zero16[16] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
 #pragma unroll
@@ -628,18 +632,25 @@ uint32_t ks_of(uint32_t w) {
 
 // Kernel-wide tile and shared-memory plan for a group sharing (ks, masked):
 // sized for the group's tallest template.
-bool make_plan(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
+bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl) {
   const uint32_t npl = masked ? 3 : 1, nacc = masked ? 2 : 1, nz = masked ? 3 : 1;
   pl.ks = ks;
   pl.masked = masked;
   pl.imgp = kM + 4 * ks + 16;
   const uint32_t kmma = 4 * ks;  // largest K of the group
   const uint32_t zplane = (kmma / 16) * (hmax + 32) * 16;
-  const uint32_t nts[2] = {masked ? 64u : 128u, 64u};
+  // tile heights, tallest first: a tile of NT output rows reads NT + h - 1
+  // image rows, so taller tiles repeat fewer rows, while the accumulators
+  // leave less tensor memory for the A stages. Binary-mask tiles of 96 rows
+  // (`tall`: launches of many tiles, where throughput counts) only where a
+  // stage still holds 3 image rows; a launch of one map or one row band ends
+  // after about one tile's time, which the 64-row tile keeps shorter.
+  const uint32_t nts[2] = {masked ? (tall ? 96u : 64u) : 128u, 64u};
   for (uint32_t nt : nts) {
     const uint32_t tm_left = kTmemCols - nacc * nt;
     const uint32_t rps = tm_left / (kStages * npl * ks);
     if (rps < 1) continue;
+    if (masked && nt > 64 && rps < 3) continue;
     const uint32_t rows = nt + hmax - 1;
     const uint32_t plane = (uint32_t)align_up((size_t)rows * pl.imgp, 128);
     for (uint32_t nbuf : {2u, 1u}) {
@@ -670,7 +681,7 @@ bool umma_supported(const MatchArgs& a) {
   if (a.mask && !a.mask_binary) return false;  // general u8 masks: CUDA-core byte planes
   if (a.w < 16 || a.h < 8 || a.h > 128 || a.w > (a.mask ? 128u : 256u) || (size_t)a.w * a.h > 33025) return false;
   UmmaPlan pl;
-  return make_plan(ks_of(a.w), a.mask != nullptr, a.h, pl);
+  return make_plan(ks_of(a.w), a.mask != nullptr, a.h, /*tall=*/false, pl);
 }
 
 uint32_t umma_group_key(const MatchArgs& a) { return ks_of(a.w) * 2 + (a.mask ? 1 : 0); }
@@ -685,7 +696,9 @@ cudaError_t umma_prepare_kernels() {
   return cudaSuccess;
 }
 
-bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) { return make_plan(ks, masked, hmax, pl); }
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
+  return make_plan(ks, masked, hmax, /*tall=*/true, pl);
+}
 
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
                          unsigned long long* ext_keys) {
@@ -751,7 +764,7 @@ cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t st
 
 cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag) {
   UmmaPlan pl;
-  if (!make_plan(ks_of(a.w), a.mask != nullptr, a.h, pl)) return cudaErrorNotSupported;
+  if (!make_plan(ks_of(a.w), a.mask != nullptr, a.h, /*tall=*/false, pl)) return cudaErrorNotSupported;
   UmmaLaunch L{};
   L.inl[0] = umma_problem(a, pl, 0, nullptr);
   L.nprobs = 1;
