@@ -258,7 +258,11 @@ ipb_status ipb_match_template_batch_device(const ipb_pair *pairs, uint32_t n,
  * the environment variable IPB_AUTOTUNE=1, else by its cost model), device
  * descriptors uploaded and the launch sequence captured in a CUDA graph.
  * Pointers in `pairs` must stay valid for the plan's life; launching replays
- * the graph on `stream`. */
+ * the graph on `stream`. Tensor-core groups run side by side inside the graph
+ * (a fork to the plan's own stream and a join back), so the launch is ordered
+ * on `stream` like one kernel. A plan holds one set of outputs and tile
+ * counters: launch it again only in stream order after the previous launch,
+ * never on two streams at once. */
 typedef struct ipb_batch_plan ipb_batch_plan;
 ipb_status ipb_batch_plan_create(const ipb_pair *pairs, uint32_t n, int precision,
                                  ipb_batch_plan **plan);
