@@ -616,6 +616,10 @@ def run_ours(args, world, rank, local):
                     "peak_note": (f"int8 dense = 2 x bf16 dense {pk['bf16_tflops']} TFLOP/s "
                                   f"({pk['source']}, MEASURED_PEAKS.json); achieved counts 2 ops "
                                   "per algorithmic MAC"),
+                    "timing_note": ("the step's two launches (unmasked and binary-mask groups) run "
+                                    "side by side on two streams and are timed as one CUDA-event "
+                                    "span on the plan's stream; launch_ms = span / 2, achieved = "
+                                    "both launches' MACs / span"),
                     "hbm_frac": (dom["algorithmic_bytes"] / dom["launches"] / per_launch_s / 1e9)
                     / pk["hbm_gbs"]}
     total_kernel_ms = sum(k["total_ms"] for k in kernels.values()) or 1.0
