@@ -100,6 +100,25 @@ def profile_collect() -> dict[str, dict]:
                                    "algorithmic_bytes": buf[k].algorithmic_bytes}
             for k in range(min(n, 32))}
 
+
+class TensorPlan(C.Structure):
+    _fields_ = [(name, C.c_uint32) for name in (
+        "tile_rows", "image_rows", "rows_per_stage", "stages", "image_buffers", "tmem_columns",
+        "smem_bytes")]
+
+
+def tensor_plan(w: int, h: int, masked: bool, batch: bool) -> dict | None:
+    """The tensor-core tile plan of a w x h template (ipb_tensor_plan_for):
+    host arithmetic, no device work. None when the tensor path does not take
+    the shape."""
+    out = TensorPlan()
+    st = lib().ipb_tensor_plan_for(w, h, int(bool(masked)), int(bool(batch)), C.byref(out))
+    if st == ERR_INVALID_ARGUMENT:
+        return None
+    check(st)
+    return {name: int(getattr(out, name)) for name, _ in TensorPlan._fields_}
+
+
 _lib = None
 
 u8p = C.POINTER(C.c_uint8)
@@ -153,6 +172,7 @@ def lib() -> C.CDLL:
     L.ipb_host_free.restype = None
     L.ipb_host_cache_release.argtypes = []
     L.ipb_host_cache_release.restype = None
+    L.ipb_tensor_plan_for.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(TensorPlan)]
     _lib = L
     return L
 

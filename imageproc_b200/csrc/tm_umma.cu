@@ -674,12 +674,18 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl)
   return false;
 }
 
+// Template shapes the tensor path takes: at least one K step of 16 bytes and
+// one 8-row band; rows within the band table; s32 sums exact (33025 pixels).
+bool umma_shape_ok(uint32_t w, uint32_t h, bool masked) {
+  return w >= 16 && h >= 8 && h <= 128 && w <= (masked ? 128u : 256u) && (size_t)w * h <= 33025;
+}
+
 }  // namespace
 
 bool umma_supported(const MatchArgs& a) {
   if (a.precision == IPB_PRECISION_REFERENCE_F32) return false;
   if (a.mask && !a.mask_binary) return false;  // general u8 masks: CUDA-core byte planes
-  if (a.w < 16 || a.h < 8 || a.h > 128 || a.w > (a.mask ? 128u : 256u) || (size_t)a.w * a.h > 33025) return false;
+  if (!umma_shape_ok(a.w, a.h, a.mask != nullptr)) return false;
   UmmaPlan pl;
   return make_plan(ks_of(a.w), a.mask != nullptr, a.h, /*tall=*/false, pl);
 }
@@ -820,3 +826,24 @@ cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const ui
 }
 
 }  // namespace ipb
+
+#define IPB_API extern "C" __attribute__((visibility("default")))
+
+IPB_API ipb_status ipb_tensor_plan_for(uint32_t w, uint32_t h, int masked, int batch, ipb_tensor_plan* out) {
+  using namespace ipb;
+  if (!out) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!umma_shape_ok(w, h, masked != 0))
+    return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "template shape not taken by the tensor path");
+  UmmaPlan pl;
+  if (!make_plan(ks_of(w), masked != 0, h, batch != 0, pl))
+    return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "no tensor-core plan fits this template");
+  const uint32_t planes = masked ? 3u : 1u, accumulators = masked ? 2u : 1u;
+  out->tile_rows = pl.NT;
+  out->image_rows = pl.NT + h - 1;
+  out->rows_per_stage = pl.rps;
+  out->stages = kStages;
+  out->image_buffers = pl.nbuf;
+  out->tmem_columns = accumulators * pl.NT + kStages * planes * pl.ks * pl.rps;
+  out->smem_bytes = pl.smem;
+  return IPB_OK;
+}

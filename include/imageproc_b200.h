@@ -272,6 +272,23 @@ ipb_status ipb_batch_plan_info(const ipb_batch_plan *plan, uint32_t *kernels,
                                uint32_t *tensor_pairs);
 ipb_status ipb_batch_plan_destroy(ipb_batch_plan *plan);
 
+/* The tensor-core tile plan that a template of w x h pixels (binary mask or
+ * not) gets: in a launch of its own (batch = 0: one map, or one row band of a
+ * host-buffer call) or in a batch-plan group (batch = 1). Host arithmetic
+ * only, no device work. Replaces no reference function: it describes this
+ * library's launches. IPB_ERR_INVALID_ARGUMENT when the tensor path does not
+ * take the shape (such templates run on CUDA cores). */
+typedef struct ipb_tensor_plan {
+    uint32_t tile_rows;      /* output rows per tile (a tile is 128 columns wide) */
+    uint32_t image_rows;     /* image rows a tile reads: tile_rows + h - 1 */
+    uint32_t rows_per_stage; /* image rows per tensor-memory pipeline stage */
+    uint32_t stages;         /* pipeline stages */
+    uint32_t image_buffers;  /* 2: the next tile's rows load during this one */
+    uint32_t tmem_columns;   /* accumulators + A stages, of the 512 per SM */
+    uint32_t smem_bytes;     /* dynamic shared memory per CTA */
+} ipb_tensor_plan;
+ipb_status ipb_tensor_plan_for(uint32_t w, uint32_t h, int masked, int batch, ipb_tensor_plan *out);
+
 /* ---- many templates against one image --------------------------------------
  * match_template (src/template_matching.rs:78-92) of n templates of one size
  * w x h against one image, unmasked, in one launch on the tensor cores
