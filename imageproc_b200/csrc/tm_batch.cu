@@ -199,6 +199,7 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     IPB_TRY(cudaEventRecord(p->ev_fork, s), "fork");
     IPB_TRY(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "fork");
   }
+  cudaError_t launch_err = cudaSuccess;
   for (size_t gi = 0; gi < p->groups.size(); ++gi) {
     const ipb_batch_plan::Group& g = p->groups[gi];
     const cudaStream_t gs = side_by_side && gi > 0 ? p->side : s;
@@ -213,7 +214,8 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     L.tag = p->tag;
     L.sched = p->d_sched + 2 * gi;
     KernelTimer* t = timed && !side_by_side ? acquire_kernel_timer() : nullptr;
-    IPB_TRY(launch_umma_batch(g.plan, L, gs, t), "tensor-core batch launch");
+    launch_err = launch_umma_batch(g.plan, L, gs, t);
+    if (launch_err != cudaSuccess) break;
     double macs = 0, bytes = 0;
     for (uint32_t i : g.members) {
       const MatchArgs& a = p->args[i];
@@ -227,9 +229,12 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     ++k;
   }
   if (side_by_side) {
+    // joined on every path, a failed launch included, so that s orders all of
+    // the side stream's work before the caller's next use of it
     IPB_TRY(cudaEventRecord(p->ev_join, p->side), "join");
     IPB_TRY(cudaStreamWaitEvent(s, p->ev_join, 0), "join");
   }
+  IPB_TRY(launch_err, "tensor-core batch launch");
   if (span) {
     timer_end(span, s);
     note_kernel_timed(span, span_macs, span_bytes);
