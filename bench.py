@@ -202,6 +202,35 @@ def cpu_reference_sample(scene, target_s: float, threads: int):
     return rows * WO * T * T * len(VARIANTS), dt, rows
 
 
+METHOD_NAMES = ["SumOfSquaredErrors", "SumOfSquaredErrorsNormalized", "CrossCorrelation",
+                "CrossCorrelationNormalized"]
+
+
+def reference_error_sample(scene, rows: int, threads: int) -> dict:
+    """The reference's own f32 error against the FP64 oracle (exact integer
+    sums, one rounding to f32) on the first `rows` output rows of each of the
+    eight score maps. The exact scores of those rows are the exact map of the
+    image rows they read, since every sum is local to its position. Scores are
+    non-negative here, so the ulp distance is the difference of the bit patterns."""
+    from oracle import oracle as O
+    image, template, mask, _ = scene
+    band = image[: rows + T - 1]
+    out = {"rows": rows, "of_rows": HO}
+    for m, masked in VARIANTS:
+        mk = mask if masked else None
+        ref = O.match_reference(image, template, m, mk, rows=(0, rows), threads=threads)
+        exact = O.match_exact(band, template, m, mk, precision=0, threads=threads)
+        rb = ref.view(np.int32).astype(np.int64)
+        eb = exact.view(np.int32).astype(np.int64)
+        ulp = np.abs(rb - eb)
+        rel = np.abs(ref.astype(np.float64) - exact.astype(np.float64)) / np.maximum(
+            np.abs(exact.astype(np.float64)), np.finfo(np.float64).tiny)
+        key = METHOD_NAMES[m] + (" masked" if masked else "")
+        out[key] = {"max_ulp": int(ulp.max()), "differing": float((ulp > 0).mean()),
+                    "max_rel": float(rel.max())}
+    return out
+
+
 def run_reference(args, world, rank):
     from imageproc_b200 import synthetic
     from oracle import oracle as O
@@ -229,6 +258,9 @@ def run_reference(args, world, rank):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        # outside the timed steps: how far the reference's f32 scores are from
+        # the FP64 oracle (the GPU arm's scores equal the oracle's bit for bit)
+        "f32_error_vs_fp64_oracle": reference_error_sample(scene, 64, threads),
     }
     print(json.dumps(line), flush=True)
 
@@ -645,6 +677,9 @@ def run_ours(args, world, rank, local):
                            "graph; e2e through match_template / match_template_with_mask with "
                            "host buffers"),
                    "parallelism": f"independent scenes per GPU x{world}"},
+        "fp64_oracle_error": ("0 ulp: all eight maps of this workload equal the FP64 oracle's bit for "
+                              "bit (tests/test_gpu_parity.py::test_blob_scene_1920x1080_template_64_exact); "
+                              "the reference arm's line reports the reference's own f32 error"),
         "queries_per_s": world * len(VARIANTS) * args.steps / (ms / 1e3),
         "graph_ms_per_step": graph_ms / args.steps,
         "roofline": roofline,
