@@ -81,6 +81,14 @@ WORKLOAD = ("blob_scene 1920x1080 u8, template 64x64, 4 methods x {unmasked, bin
             "Bernoulli(0.8)}: 8 score maps 1857x1017 f32 per step")
 
 
+def bench_config() -> dict:
+    """The workload both arms time (the same dict in both lines); how each arm
+    computes it goes in the line's `arm` object."""
+    return {"workload": WORKLOAD, "maps_per_step": len(VARIANTS), "mac_per_step": MAC_PER_STEP,
+            "baseline_config": 2,
+            "l2": "GPU arm: flushed between steps (256 MiB write, outside the timed events)"}
+
+
 def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -254,7 +262,10 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
+        "data": "synthetic", "config": bench_config(),
+        "arm": {"precision": "the reference's f32 accumulation and normalisation",
+                "api": "oracle restatement of the reference's per-pixel loop (match_template_parallel)",
+                "parallelism": f"rows over {threads} host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -669,14 +680,14 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "flushed between steps (256 MiB write)",
-                   "precision": "exact integer sums, FP64 normalisation",
-                   "api": ("ipb_batch_plan_launch: one persistent tcgen05 launch per mask kind "
-                           "(4 maps each), run eagerly in the timed region so CUDA events bracket "
-                           "each kernel; graph_ms_per_step is the same plan replayed as a CUDA "
-                           "graph; e2e through match_template / match_template_with_mask with "
-                           "host buffers"),
-                   "parallelism": f"independent scenes per GPU x{world}"},
+        "config": bench_config(),
+        "arm": {"precision": "exact integer sums, FP64 normalisation",
+                "api": ("ipb_batch_plan_launch: one persistent tcgen05 launch per mask kind "
+                        "(4 maps each), run eagerly in the timed region so CUDA events bracket "
+                        "each kernel; graph_ms_per_step is the same plan replayed as a CUDA "
+                        "graph; e2e through match_template / match_template_with_mask with "
+                        "host buffers"),
+                "parallelism": f"independent scenes per GPU x{world}"},
         "fp64_oracle_error": ("0 ulp: all eight maps of this workload equal the FP64 oracle's bit for "
                               "bit (tests/test_gpu_parity.py::test_blob_scene_1920x1080_template_64_exact); "
                               "the reference arm's line reports the reference's own f32 error"),

@@ -173,6 +173,8 @@ def lib() -> C.CDLL:
     L.ipb_host_cache_release.argtypes = []
     L.ipb_host_cache_release.restype = None
     L.ipb_tensor_plan_for.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(TensorPlan)]
+    L.ipb_debug_set_pipeline_wait_ns.argtypes = [C.c_uint64]
+    L.ipb_debug_set_pipeline_wait_ns.restype = None
     _lib = L
     return L
 

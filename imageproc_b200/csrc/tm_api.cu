@@ -103,6 +103,26 @@ void count_launch(int id) {
 }
 
 namespace {
+std::atomic<unsigned long long> g_wait_ns{kDefaultWaitNs};
+}  // namespace
+
+unsigned long long pipeline_wait_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+
+int device_sm_count() {
+  static std::atomic<int> cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev >= 0 && dev < 64) {
+    const int n = cache[dev].load(std::memory_order_relaxed);
+    if (n > 0) return n;
+  }
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  if (dev >= 0 && dev < 64) cache[dev].store(n, std::memory_order_relaxed);
+  return n;
+}
+
+namespace {
 
 thread_local std::string g_last_error;
 
@@ -642,6 +662,10 @@ IPB_API ipb_status ipb_set_precision(int precision) {
 }
 
 IPB_API int ipb_get_precision(void) { return g_precision.load(); }
+
+IPB_API void ipb_debug_set_pipeline_wait_ns(uint64_t ns) {
+  g_wait_ns.store(ns ? (unsigned long long)ns : kDefaultWaitNs, std::memory_order_relaxed);
+}
 
 IPB_API ipb_status ipb_set_path(int path) {
   if (path < 0 || path > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown kernel path");

@@ -212,6 +212,7 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     L.tiles = g.tiles;
     L.err = p->d_err;
     L.tag = p->tag;
+    L.wait_ns = pipeline_wait_ns();
     L.sched = p->d_sched + 2 * gi;
     KernelTimer* t = timed && !side_by_side ? acquire_kernel_timer() : nullptr;
     launch_err = launch_umma_batch(g.plan, L, gs, t);

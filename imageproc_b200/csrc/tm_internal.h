@@ -1,11 +1,52 @@
 // tm_internal.h -- launchers shared between the kernel files and the C ABI.
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 namespace ipb {
+
+// ---- per-device one-time set-up ------------------------------------------------
+// A kernel's dynamic shared-memory limit (cudaFuncSetAttribute) belongs to the
+// current device's context, not to the process: a process that uses two GPUs
+// must set it on each. run(f) calls f() the first time it is reached with a
+// given device current and returns cudaSuccess afterwards for that device; a
+// failing f is tried again on the next call. Safe to call from many threads.
+class PerDeviceOnce {
+ public:
+  template <typename F>
+  cudaError_t run(F&& f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return f();  // beyond the bitmask: set every time
+    const uint64_t bit = 1ull << dev;
+    if (done_.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    std::lock_guard<std::mutex> g(mu_);
+    if (done_.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+    e = f();
+    if (e == cudaSuccess) done_.fetch_or(bit, std::memory_order_release);
+    return e;
+  }
+
+ private:
+  std::atomic<uint64_t> done_{0};
+  std::mutex mu_;
+};
+
+// Streaming multiprocessors of the current device (cached per device).
+int device_sm_count();
+
+// Budget, in nanoseconds, of the bounded waits inside each tile of the
+// tensor-core kernels (default 2 s). A wait that runs out stops the kernel's
+// pipeline and reports IPB_ERR_TIMEOUT; the final wait for in-flight
+// tensor-core work before tensor memory is freed always keeps the default.
+// Lowered only by the test entry point ipb_debug_set_pipeline_wait_ns.
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
+unsigned long long pipeline_wait_ns();
 
 // ---- tracing ---------------------------------------------------------------
 // Every kernel launch site reports itself; the C ABI exposes the running
@@ -162,6 +203,8 @@ struct UmmaLaunch {
   uint32_t z_off, img_off, rs_off;
   unsigned int* err;
   unsigned int tag;
+  // budget of the pipeline's bounded waits, per tile (pipeline_wait_ns())
+  unsigned long long wait_ns;
   // {next tile counter, CTAs finished}, both zero at launch: tiles after the
   // first wave are claimed from it; the last CTA out zeroes it again.
   // Null: a fixed grid stride.

@@ -52,7 +52,7 @@ constexpr int kPosW = kM / kEpiPerQuad;         // templates as M: positions per
 constexpr int kThreads = (kMmaWarp + 1) * 32;
 constexpr int kStrips = 3;
 constexpr uint32_t kTmemCols = 256;  // two accumulators of up to 128 columns
-constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr unsigned long long kWaitNs = kDefaultWaitNs;  // the final drain's budget
 
 struct ManyParams {
   const uint8_t* img;
@@ -72,6 +72,7 @@ struct ManyParams {
   unsigned long long* ext;    // 2 keys per template or null
   unsigned int* err;
   unsigned int tag;
+  unsigned long long wait_ns;  // budget of the bounded waits per tile (pipeline_wait_ns())
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
       }
     }
     __syncthreads();
-    const unsigned long long deadline = global_ns() + kWaitNs;
+    const unsigned long long deadline = global_ns() + p.wait_ns;
 
     if (warp < kBuildWarps) {
       // strips: S_x[j][rho] = image row rho, bytes [xi + 16j, xi + 16j + 16)
@@ -537,16 +538,7 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
   }
 }
 
-int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int sm_count() { return device_sm_count(); }
 
 __global__ void many_keys_init_kernel(unsigned long long* keys, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -656,16 +648,17 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   p.ext = ext_keys;
   p.err = err;
   p.tag = tag;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(many_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  p.wait_ns = pipeline_wait_ns();
+  static PerDeviceOnce attr;
+  cudaError_t e = attr.run([] {
+    cudaError_t r = cudaFuncSetAttribute(many_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSmemLimit);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(many_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (r == cudaSuccess)
+      r = cudaFuncSetAttribute(many_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kSmemLimit);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+    return r;
+  });
+  if (e != cudaSuccess) return e;
   // CTAs come in groups of nblocks (one per template block)
   uint32_t per = (uint32_t)sm_count() / p.nblocks;
   if (per < 1) per = 1;

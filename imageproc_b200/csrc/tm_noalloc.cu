@@ -4,8 +4,9 @@
 // that owns the whole device-memory budget, a latency-critical loop in which
 // cudaMalloc/cudaFree would stall or synchronise the device, or code that must
 // not meet an out-of-memory failure after start-up. For them,
-// ipb_match_template_device_noalloc runs the same kernels as
-// ipb_match_template_device, but its scratch memory (template planes, the
+// ipb_match_template_device_noalloc runs the CUDA-core kernels of
+// ipb_match_template_device (never the tensor-core kernel, whose shapes it
+// therefore runs slower, with the same scores), and its scratch memory (template planes, the
 // template constant and the u64 integral image of I^2) lives in one fixed
 // array compiled into this library instead of a buffer obtained at run time.
 //
@@ -14,7 +15,8 @@
 // Host code cannot use the array's name as a device address, so the first call
 // on each device looks the address up with cudaGetSymbolAddress (with that
 // device current) and caches it; make that first call before any stream
-// capture. All calls share the one array and it keeps whatever the last call
+// capture. The cached address is not looked up again, so calls after a
+// cudaDeviceReset of that device are not supported. All calls share the one array and it keeps whatever the last call
 // left there: the kernels clear what must start at zero on every call, and two
 // calls that overlap on the GPU (different streams, or different host threads
 // on the same device) race on it, so callers must order them.

@@ -68,7 +68,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kStages = 2;  // A-row stages in tensor memory
 constexpr uint32_t kMaxRps = 16;
 constexpr uint32_t kTmemCols = 512;
-constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr unsigned long long kWaitNs = kDefaultWaitNs;  // the final drain's budget
 constexpr uint32_t kBandTable = 1024;          // per-row MMA band table (uint4 per image row)
 constexpr uint32_t kMaxTileRows = 256;         // NT + h - 1 <= 128 + 128 - 1
 constexpr uint32_t kSmemHeader = kBandTable + kMaxTileRows * 16;
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       issue_tile_load(L, P[pn], s_img + (buf ^ 1u) * NPL * L.plane_bytes, next - P[pn].tile_begin);
     }
     const uint32_t nst = (nrows + L.rps - 1) / L.rps;
-    const unsigned long long deadline = global_ns() + kWaitNs;
+    const unsigned long long deadline = global_ns() + L.wait_ns;
 
     if (!mma_warp) {
       // builder warp: lane quadrant q4 of tensor memory, sub-group sub (kSubs per quadrant)
@@ -464,6 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         const uint32_t s = g % kStages;
         const bool got = g < kStages || mbar_wait_sleep(&empty[s], ((g / kStages) + 1) & 1u, deadline);
         if (!__all_sync(0xffffffffu, got)) {  // warp-uniform: the warp arrives as one below
+          tmem_wait_st();  // the tile's zeroing stores land before tensor memory can be freed
           ok = false;
           break;
         }
@@ -595,13 +596,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
 
 template <int KS, bool MASKED>
 cudaError_t launch_ks(const UmmaLaunch& L, uint32_t smem, uint32_t grid, cudaStream_t s) {
-  static bool attr_set = false;  // per instantiation, process-wide
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static PerDeviceOnce attr;  // per instantiation and device
+  cudaError_t e = attr.run([] {
+    return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                227 * 1024);
+  });
+  if (e != cudaSuccess) return e;
   umma_match_kernel<KS, MASKED><<<grid, kThreads, smem, s>>>(L);
   return cudaGetLastError();
 }
@@ -612,16 +612,7 @@ cudaError_t set_smem_attr() {
                               227 * 1024);
 }
 
-int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int sm_count() { return device_sm_count(); }
 
 uint32_t ks_of(uint32_t w) {
   const uint32_t kmma = (w + 31) & ~31u;
@@ -777,6 +768,7 @@ cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int
   L.tiles = umma_problem_tiles(L.inl[0], pl);
   L.err = err_word;
   L.tag = tag;
+  L.wait_ns = pipeline_wait_ns();
   return launch_umma_batch(pl, L, a.stream, a.timer);
 }
 

@@ -131,6 +131,17 @@ int ipb_get_precision(void);
 ipb_status ipb_set_path(int path);
 int ipb_get_path(void);
 
+/* Failure-detection test hook (no counterpart in the reference): the budget,
+ * in nanoseconds, of the bounded waits inside each tile of the tensor-core
+ * kernels; 0 restores the default of 2 s. A wait that runs out stops the
+ * kernel's pipeline, lets its tensor-core work drain (that last wait keeps the
+ * 2 s budget), frees its tensor memory and makes the call report
+ * IPB_ERR_TIMEOUT; the context stays usable. Takes effect for launches
+ * planned after the call (batch plans keep the budget they were made with).
+ * Tests set a budget far below one tile's time to make a wait run out without
+ * faulting or hanging the GPU. */
+void ipb_debug_set_pipeline_wait_ns(uint64_t ns);
+
 /* ---- tracing -------------------------------------------------------------
  * No counterpart in the reference (which has no instrumentation); used by the
  * benchmark and the profiling notes. */
@@ -208,14 +219,18 @@ ipb_status ipb_match_template_device(
  * inside an application that owns the device-memory budget, a latency-critical
  * loop where cudaMalloc/cudaFree would stall or synchronise the device, code
  * that must not hit an out-of-memory failure after start-up). Same arguments
- * and results as ipb_match_template_device; the caller still passes inputs and
- * outputs. Its scratch memory is a fixed 16 MiB array inside the library,
+ * and the same scores as ipb_match_template_device; the caller still passes
+ * inputs and outputs. It runs the CUDA-core kernels only (no tensor-core
+ * path), so large templates can take several times longer than through
+ * ipb_match_template_device. Its scratch memory is a fixed 16 MiB array inside the library,
  * which every GPU that loads the library holds until the process exits;
  * problems needing more (the u64 integral image of an unmasked SSE or
  * normalised match takes (W+1)(H+1)*8 bytes, so images up to about 2.09
  * megapixels) fail with IPB_ERR_INVALID_ARGUMENT and a message naming the
  * size. The first call on each device looks up the array's device address
- * (make it before any stream capture). All calls share the array: calls that
+ * (make it before any stream capture) and keeps it for the life of the
+ * process, so a device reset (cudaDeviceReset) is not supported afterwards,
+ * as for the rest of this library. All calls share the array: calls that
  * overlap on the GPU race on it and must be ordered by the caller. */
 ipb_status ipb_match_template_device_noalloc(
     const uint8_t *d_image, uint32_t image_width, uint32_t image_height,

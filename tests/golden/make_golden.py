@@ -8,19 +8,20 @@ values that the tests build with f32 expressions such as
 ``14.0 / (22.0 * tss).sqrt()`` are evaluated with numpy float32 arithmetic,
 which rounds each operation like Rust's f32.
 
-Usage: python tests/golden/make_golden.py [path/to/template_matching.rs]
+Usage: python tests/golden/make_golden.py path/to/imageproc/src/template_matching.rs
+(or set IMAGEPROC_SRC to the imageproc source directory)
 """
 
 from __future__ import annotations
 
 import json
 import re
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
-DEFAULT_SRC = Path("/root/reference/src/template_matching.rs")
 OUT = Path(__file__).with_name("reference_unit_tests.json")
 REL = "src/template_matching.rs"
 
@@ -174,4 +175,9 @@ def main(src: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_SRC)
+    if len(sys.argv) > 1:
+        main(Path(sys.argv[1]))
+    elif os.environ.get("IMAGEPROC_SRC"):
+        main(Path(os.environ["IMAGEPROC_SRC"]) / "template_matching.rs")
+    else:
+        sys.exit(__doc__)

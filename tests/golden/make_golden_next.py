@@ -9,17 +9,18 @@ compiled or run: the ``gray_image!`` / ``rgb_image!`` literals, the
 ``sum_image_pixels`` assertions, the ``put_pixel`` calls and the ``T::new``
 point lists are parsed.
 
-Usage: python tests/golden/make_golden_next.py [path/to/imageproc/src]
+Usage: python tests/golden/make_golden_next.py path/to/imageproc/src
+(or set IMAGEPROC_SRC to that directory)
 """
 
 from __future__ import annotations
 
 import json
 import re
+import os
 import sys
 from pathlib import Path
 
-DEFAULT_SRC = Path("/root/reference/src")
 OUT = Path(__file__).with_name("reference_next_tests.json")
 
 
@@ -148,7 +149,12 @@ def filter_tests(src: str) -> list[dict]:
 
 
 def main() -> None:
-    src = Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_SRC
+    if len(sys.argv) > 1:
+        src = Path(sys.argv[1])
+    elif os.environ.get("IMAGEPROC_SRC"):
+        src = Path(os.environ["IMAGEPROC_SRC"])
+    else:
+        sys.exit(__doc__)
     data = {
         "reference": "image-rs/imageproc 0.27.0",
         "integral_image": {"file": "src/integral_image.rs",
