@@ -41,6 +41,10 @@ def lib() -> C.CDLL:
         L.tmo_sums.argtypes = [u8p, u32, u32, u8p, u32, u32, u8p, u64p, u64p, u64p, C.c_int]
         L.tmo_match_exact.argtypes = [u8p, u32, u32, u8p, u32, u32, u8p, u32, u32, C.c_int, C.c_int,
                                       f32p, C.c_int]
+        L.tmo_match_exact_fast.argtypes = [u8p, u32, u32, u8p, u32, u32, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_void_p, C.c_int]
+        L.tmo_many_exact_fast.argtypes = [u8p, u32, u32, u8p, u32, u32, u32, C.c_int, C.c_int,
+                                          u32, u32, C.c_void_p, C.c_void_p, C.c_int]
         L.tmo_finish.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64]
         L.tmo_finish.restype = C.c_float
         L.tmo_find_extremes_index.argtypes = [C.c_void_p, u32, u32, C.c_int,
@@ -122,6 +126,55 @@ def match_exact(image, template, method, mask=None, precision=0, threads=None) -
     if st:
         raise OracleError(f"oracle status {st}")
     return out
+
+
+class _Extremes(C.Structure):
+    _fields_ = [("max_value", C.c_double), ("min_value", C.c_double),
+                ("max_x", C.c_uint32), ("max_y", C.c_uint32),
+                ("min_x", C.c_uint32), ("min_y", C.c_uint32)]
+
+
+def match_exact_fast(image, template, method, precision=0, want_map=True, threads=None):
+    """Unmasked exact scores through the fast oracle form (templates of at most
+    66051 pixels): returns (map or None, extremes) where extremes is
+    find_extremes of the f32 map, (max_value, min_value, (max_x, max_y),
+    (min_x, min_y)). The scores equal match_exact's."""
+    image = np.ascontiguousarray(image, dtype=np.uint8)
+    template = np.ascontiguousarray(template, dtype=np.uint8)
+    H, W = image.shape
+    h, w = template.shape
+    out = np.empty((H - h + 1, W - w + 1), np.float32) if want_map else None
+    ext = _Extremes()
+    st = lib().tmo_match_exact_fast(_p(image), W, H, _p(template), w, h, int(method),
+                                    int(precision), _p(out), C.byref(ext),
+                                    threads if threads is not None else default_threads())
+    if st:
+        raise OracleError(f"oracle status {st}")
+    e = (np.float32(ext.max_value), np.float32(ext.min_value), (ext.max_x, ext.max_y),
+         (ext.min_x, ext.min_y))
+    return out, e
+
+
+def many_exact_fast(image, templates, method, precision=0, rows=None, want_maps=False,
+                    threads=None):
+    """n unmasked templates of one size (an (n, h, w) u8 array) against one
+    image through the fast oracle form, output rows [r0, r1) (default all).
+    Returns (maps or None, extremes): maps (n, r1 - r0, Wo) f32, extremes a
+    list of n find_extremes tuples over those rows, in full-map coordinates."""
+    image = np.ascontiguousarray(image, dtype=np.uint8)
+    templates = np.ascontiguousarray(templates, dtype=np.uint8)
+    H, W = image.shape
+    n, h, w = templates.shape
+    r0, r1 = rows if rows is not None else (0, H - h + 1)
+    maps = np.empty((n, r1 - r0, W - w + 1), np.float32) if want_maps else None
+    ext = (_Extremes * n)()
+    st = lib().tmo_many_exact_fast(_p(image), W, H, _p(templates), w, h, n, int(method),
+                                   int(precision), r0, r1, _p(maps), ext,
+                                   threads if threads is not None else default_threads())
+    if st:
+        raise OracleError(f"oracle status {st}")
+    return maps, [(np.float32(e.max_value), np.float32(e.min_value), (e.max_x, e.max_y),
+                   (e.min_x, e.min_y)) for e in ext]
 
 
 def find_extremes(image):

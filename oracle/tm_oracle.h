@@ -68,11 +68,37 @@ int tmo_match_exact(const uint8_t *image, uint32_t W, uint32_t H,
                     const uint8_t *mask, uint32_t mw, uint32_t mh,
                     int method, int precision, float *out, int nthreads);
 
+struct tmo_extremes_s;
+
+/* Fast form of tmo_match_exact for UNMASKED templates of at most 66051
+ * pixels (so every X = sum(I*T) fits u32), for the full-size parity checks:
+ * X accumulated per output row in u32 with a vectorisable inner loop, Y from
+ * the exact u64 integral image of I^2, the same tmo_finish epilogue. The
+ * scores equal tmo_match_exact's (tests/test_oracle_fast.py checks this).
+ * out (the Wo x Ho map) may be NULL; ext, when not NULL, receives
+ * find_extremes of the f32 map (first occurrence in row-major order; the
+ * map has no NaN). Returns TMO_ERR_INVALID_ARGUMENT for larger templates. */
+int tmo_match_exact_fast(const uint8_t *image, uint32_t W, uint32_t H,
+                         const uint8_t *templ, uint32_t w, uint32_t h,
+                         int method, int precision, float *out,
+                         struct tmo_extremes_s *ext, int nthreads);
+
+/* The same for n unmasked templates of one size (back to back in
+ * `templates`) against one image, output rows [row_begin, row_end) only:
+ * out (NULL allowed) receives n template-major maps of
+ * (row_end - row_begin) x Wo scores, ext (NULL allowed) n records of
+ * find_extremes over those rows, locations in full-map coordinates. */
+int tmo_many_exact_fast(const uint8_t *image, uint32_t W, uint32_t H,
+                        const uint8_t *templates, uint32_t w, uint32_t h,
+                        uint32_t n, int method, int precision,
+                        uint32_t row_begin, uint32_t row_end, float *out,
+                        struct tmo_extremes_s *ext, int nthreads);
+
 /* One output from exact sums (the epilogue the GPU kernels must match). */
 float tmo_finish(int method, int precision, uint64_t X, uint64_t Y,
                  uint64_t tss);
 
-typedef struct {
+typedef struct tmo_extremes_s {
     double max_value, min_value;
     uint32_t max_x, max_y, min_x, min_y;
 } tmo_extremes;
