@@ -93,7 +93,7 @@ const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
       "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress", "filter",
-      "example"};
+      "example", "proposal_net", "propose"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 

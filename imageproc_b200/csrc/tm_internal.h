@@ -65,6 +65,8 @@ enum KernelId : int {
   kKernelSuppress,
   kKernelFilter,
   kKernelExample,
+  kKernelLearned,
+  kKernelPropose,
   kKernelCount
 };
 const char* kernel_name(int id);

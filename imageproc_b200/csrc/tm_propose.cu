@@ -1,0 +1,831 @@
+// tm_propose.cu -- learned proposals, exact verification and certification
+// for many 48 x 48 templates against one large image (SumOfSquaredErrors).
+//
+// The reference answers "where does this template match best" by scoring
+// every window (match_template, src/template_matching.rs:78-92) and taking
+// find_extremes (:479-511): the first minimum in row-major order. Here:
+//   1. the proposal network (tm_learned.cuh) scores every downsampled
+//      position for every template: the heatmap z_t(p), reduced on the fly
+//      to the maximum of each 8 x 8 cell (head_cells_kernel, bf16 tensor
+//      cores, fp32 accumulation);
+//   2. per template, the top-k cells and a confidence margin: the softmax
+//      probability of the best cell minus that of the best cell not next to
+//      it (topk_kernel);
+//   3. a window of 32 x 32 positions around each proposal is scored exactly
+//      (integer sums, the many-templates kernel's f32 rounding) and the first
+//      minimum kept (verify_kernel);
+//   4. certification: for SumOfSquaredErrors every window p satisfies
+//      SSE(p) >= sum_b (S_I,b(p) - S_T,b)^2 / 144 over the 16 blocks b of
+//      12 x 12 pixels of the template (Cauchy-Schwarz on each block), with
+//      S the block sums. Over a block of positions, S_I,b lies between the
+//      minimum and maximum of the image's 12 x 12 box sums there, which gives
+//      a lower bound for the whole block from two tables built once per
+//      image. Blocks whose bound exceeds the verified minimum cannot hold the
+//      answer; the others must lie inside a verified window, or are verified
+//      too (up to a budget) -- otherwise the template falls back;
+//   5. templates whose margin is below the threshold, or that could not be
+//      certified, are answered by the exhaustive many-templates kernel.
+// A certified answer equals find_extremes' minimum of the exhaustive map
+// exactly: every position outside the verified set has a larger score.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "imageproc_b200.h"
+#include "tm_internal.h"
+#include "tm_learned.cuh"
+
+#define IPB_API extern "C" __attribute__((visibility("default")))
+
+namespace ipb {
+namespace learned {
+namespace {
+
+constexpr int kCell = 8;          // heatmap cell: 8 x 8 downsampled positions
+constexpr int kMaxTopK = 32;
+constexpr int kWin = 32;          // verification window: 32 x 32 positions
+constexpr int kBlk = 12;          // certification block: 12 x 12 positions
+constexpr int kMaxExtra = 256;    // most extra blocks a template may verify
+constexpr int kPatch = kWin + kTpl - 1;        // 79 image rows / columns per window
+constexpr int kPatchPitch = 96;                // 16-byte multiple >= kPatch + 4
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+__host__ __device__ __forceinline__ uint16_t f2bf(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+// f32 bits -> unsigned key with the same order (no NaNs here)
+__host__ __device__ __forceinline__ uint32_t okey(float f) {
+  uint32_t b;
+  memcpy(&b, &f, 4);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float okey_value(uint32_t k) {
+  const uint32_t b = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+// ---- 1. heatmap cells --------------------------------------------------------------
+// Block: 8 downsampled rows (one cell row) x 64 positions x 32 templates; warp
+// w takes row w, four 16-position m-tiles and four 8-template n-tiles; the
+// "taps" are the four offsets o of the 2x2 embedding.
+constexpr int kHW = 64, kHInW = kHW + 1, kGPitch = 40;
+struct HeadSmem {
+  uint4 in[kCell + 1][kChunks][kHInW];   // 37440 B
+  uint16_t g[4][32][kGPitch];            // 10240 B
+};
+
+__global__ void __launch_bounds__(256) head_cells_kernel(const uint4* __restrict__ F, uint32_t H, uint32_t W,
+                                                         const uint16_t* __restrict__ gb, uint32_t T,
+                                                         unsigned long long* __restrict__ cells) {
+  __shared__ __align__(16) HeadSmem sm;
+  const int y0 = blockIdx.y * kCell, x0 = blockIdx.x * kHW;
+  const uint32_t t0 = blockIdx.z * 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < (kCell + 1) * kChunks * kHInW; i += 256) {
+    const int px = i % kHInW, c = (i / kHInW) % kChunks, r = i / (kHInW * kChunks);
+    const int y = y0 + r, x = x0 + px;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (y < (int)H && x < (int)W) v = F[((size_t)y * kChunks + c) * W + x];
+    sm.in[r][c][px] = v;
+  }
+  for (int i = tid; i < 4 * 32 * 4; i += 256) {  // 4 offsets x 32 templates x 4 chunks of 8 channels
+    const int q = i & 3, row = i >> 2, o = row / 32, tl = row % 32;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (t0 + tl < T) v = reinterpret_cast<const uint4*>(gb)[((size_t)o * T + t0 + tl) * 4 + q];
+    *reinterpret_cast<uint4*>(&sm.g[o][tl][8 * q]) = v;
+  }
+  __syncthreads();
+
+  float acc[4][4][4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[m][j][e] = 0.f;
+  const int lrow = lane & 7, lm = lane >> 3;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const int oy = o >> 1, ox = o & 1;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      uint32_t b[4][2];
+#pragma unroll
+      for (int jp = 0; jp < 2; ++jp) {
+        const int tl = 8 * (2 * jp + (lm >> 1)) + lrow;
+        ldsm_x4(smem_addr(&sm.g[o][tl][8 * (2 * s + (lm & 1))]), b[2 * jp][0], b[2 * jp][1], b[2 * jp + 1][0],
+                b[2 * jp + 1][1]);
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        uint32_t a0, a1, a2, a3;
+        const int px = 16 * m + ox + lrow + 8 * (lm & 1);
+        ldsm_x4(smem_addr(&sm.in[warp + oy][2 * s + (lm >> 1)][px]), a0, a1, a2, a3);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[m][j], a0, a1, a2, a3, b[j][0], b[j][1]);
+      }
+    }
+  }
+  // cell maxima: (order key of the logit, complement of the position) so that
+  // ties go to the smaller position; the staged input is dead, so the cell
+  // table lives in its first 2 KB
+  __syncthreads();
+  unsigned long long (*cell)[32] = reinterpret_cast<unsigned long long (*)[32]>(&sm.in[0][0][0]);
+  for (int i = tid; i < (kHW / kCell) * 32; i += 256) (&cell[0][0])[i] = 0ull;
+  __syncthreads();
+  const int g = lane >> 2, t = lane & 3;
+  const int y = y0 + warp;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int x = x0 + 16 * m + g + 8 * (e >> 1);
+        unsigned long long key = 0ull;
+        if (y < (int)H && x < (int)W)
+          key = ((unsigned long long)okey(kAlpha * acc[m][j][e]) << 32) |
+                (0xFFFFFFFFu - (uint32_t)((uint32_t)y * W + (uint32_t)x));
+#pragma unroll
+        for (int d = 4; d < 32; d <<= 1) {
+          const unsigned long long o2 = __shfl_xor_sync(0xffffffffu, key, d);
+          key = o2 > key ? o2 : key;
+        }
+        if (g == 0) atomicMax(&cell[2 * m + (e >> 1)][8 * j + 2 * t + (e & 1)], key);
+      }
+  __syncthreads();
+  const uint32_t Cx = (W + kCell - 1) / kCell, Cy = (H + kCell - 1) / kCell;
+  for (int i = tid; i < (kHW / kCell) * 32; i += 256) {
+    const int tl = i / (kHW / kCell), cl = i % (kHW / kCell);
+    const uint32_t cx = blockIdx.x * (kHW / kCell) + cl, cy = blockIdx.y;
+    if (t0 + tl < T && cx < Cx && cy < Cy) cells[((size_t)(t0 + tl) * Cy + cy) * Cx + cx] = cell[cl][tl];
+  }
+}
+
+// G (fp32, [T][o * 32 + c]) -> bf16 [o][T][c] for the head's B operand
+__global__ void pack_embedding_kernel(const float* __restrict__ G, uint32_t T, uint16_t* __restrict__ gb) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T * kEmb) return;
+  const uint32_t t = i / kEmb, o = (i % kEmb) / kC, c = i % kC;
+  gb[((size_t)o * T + t) * kC + c] = f2bf(G[i]);
+}
+
+// ---- 2. top-k cells and margin ----------------------------------------------------
+struct TopK {
+  uint32_t pos[kMaxTopK];  // downsampled positions (y * W + x) of the best cells
+  float logit[kMaxTopK];
+  float margin;
+  uint32_t count;
+};
+
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
+  for (int d = 16; d; d >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, d);
+    v = o > v ? o : v;
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0ull;
+    for (int d = 16; d; d >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, d);
+      v = o > v ? o : v;
+    }
+    if (threadIdx.x == 0) red[32] = v;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+__device__ __forceinline__ float block_sum(float v, float* red) {
+  for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    if (threadIdx.x == 0) red[32] = v;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// One block (1024 threads) per template: repeated block maxima over the cells
+// (a selected cell is excluded by its index), then the softmax over all cells.
+__global__ void __launch_bounds__(1024) topk_kernel(const unsigned long long* __restrict__ cells, uint32_t Cy,
+                                                    uint32_t Cx, uint32_t W, uint32_t k, TopK* __restrict__ out) {
+  __shared__ unsigned long long red[33];
+  __shared__ float redf[33];
+  __shared__ uint32_t sel_cell[kMaxTopK];
+  const unsigned long long* ct = cells + (size_t)blockIdx.x * Cy * Cx;
+  const uint32_t nc = Cy * Cx;
+  TopK r;
+  r.count = 0;
+  for (uint32_t round = 0; round < k; ++round) {
+    unsigned long long best = 0ull;
+    uint32_t best_i = 0xFFFFFFFFu;
+    for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
+      bool taken = false;
+      for (uint32_t q = 0; q < round; ++q) taken |= sel_cell[q] == i;
+      const unsigned long long v = taken ? 0ull : ct[i];
+      if (v > best) {
+        best = v;
+        best_i = i;
+      }
+    }
+    const unsigned long long m = block_max_u64(best, red);
+    if (m == 0ull) break;
+    // the owner of the maximum records its cell (keys are distinct: they hold the position)
+    if (best == m) sel_cell[round] = best_i;
+    __syncthreads();
+    r.pos[round] = 0xFFFFFFFFu - (uint32_t)(m & 0xFFFFFFFFu);
+    r.logit[round] = okey_value((uint32_t)(m >> 32));
+    r.count = round + 1;
+  }
+  // margin: softmax probability of the best cell minus that of the best cell
+  // that is not one of its 8 neighbours
+  float margin = 0.f;
+  if (r.count > 0) {
+    const float z1 = r.logit[0];
+    const uint32_t c1 = sel_cell[0], cy1 = c1 / Cx, cx1 = c1 % Cx;
+    float se = 0.f;
+    unsigned long long far = 0ull;
+    for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
+      const unsigned long long v = ct[i];
+      se += expf(okey_value((uint32_t)(v >> 32)) - z1);
+      const uint32_t cy = i / Cx, cx = i % Cx;
+      const bool near = (cy + 1 >= cy1 && cy <= cy1 + 1 && cx + 1 >= cx1 && cx <= cx1 + 1);
+      if (!near && v > far) far = v;
+    }
+    const float S = block_sum(se, redf);
+    const unsigned long long f2 = block_max_u64(far, red);
+    const float p2 = f2 ? expf(okey_value((uint32_t)(f2 >> 32)) - z1) / S : 0.f;
+    margin = 1.f / S - p2;
+  }
+  r.margin = margin;
+  if (threadIdx.x == 0) out[blockIdx.x] = r;
+  (void)W;
+}
+
+// ---- 3. exact verification of rectangles of positions ------------------------------------
+struct Rect {
+  uint32_t x0, y0, w, h;  // positions [x0, x0 + w) x [y0, y0 + h), w, h <= 32
+};
+
+// One block per (rectangle, template): the image patch and the template in
+// shared memory; thread (row r, 4-position group) sums X = sum I*T with dp4a
+// over aligned image words shifted by byte_perm, Y from row prefix sums of
+// I^2, and SSE = Y - 2X + TSS in integers, rounded once to f32 (the
+// many-templates kernel's EXACT_FP64 SumOfSquaredErrors). The first minimum
+// (order key of the score, then the position index) goes to best[t].
+__global__ void __launch_bounds__(256) verify_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
+                                                     const uint8_t* __restrict__ tpl, const Rect* __restrict__ rects,
+                                                     const uint32_t* __restrict__ counts, uint32_t max_rects,
+                                                     unsigned long long* __restrict__ best) {
+  __shared__ __align__(16) uint8_t s_img[kPatch][kPatchPitch];
+  __shared__ uint32_t s_tpl[kTpl][kTpl / 4];
+  __shared__ uint32_t s_sq[kPatch][kPatch + 1];  // prefix sums of I^2 per row
+  __shared__ unsigned long long s_best[8];
+  __shared__ unsigned long long s_tss;
+  const uint32_t t = blockIdx.y;
+  if (blockIdx.x >= counts[t]) return;
+  const Rect rc = rects[(size_t)t * max_rects + blockIdx.x];
+  const uint32_t Wo = W - kTpl + 1;
+  const uint8_t* tp = tpl + (size_t)t * kTpl * kTpl;
+  const uint32_t pw = rc.w + kTpl - 1, ph = rc.h + kTpl - 1;
+  for (uint32_t i = threadIdx.x; i < ph * kPatchPitch; i += blockDim.x) {
+    const uint32_t r = i / kPatchPitch, c = i % kPatchPitch;
+    s_img[r][c] = (c < pw) ? img[(size_t)(rc.y0 + r) * W + rc.x0 + c] : 0;
+  }
+  for (uint32_t i = threadIdx.x; i < kTpl * kTpl / 4; i += blockDim.x)
+    s_tpl[i / (kTpl / 4)][i % (kTpl / 4)] = reinterpret_cast<const uint32_t*>(tp)[i];
+  if (threadIdx.x == 0) s_tss = 0ull;
+  __syncthreads();
+  {
+    unsigned long long part = 0ull;
+    for (uint32_t i = threadIdx.x; i < kTpl * kTpl; i += blockDim.x) {
+      const uint32_t v = tp[i];
+      part += v * v;
+    }
+    for (int d = 16; d; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_tss, part);
+  }
+  // row prefix sums of I^2 (one warp per row)
+  for (uint32_t r = threadIdx.x >> 5; r < ph; r += blockDim.x >> 5) {
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < pw; c0 += 32) {
+      const uint32_t c = c0 + (threadIdx.x & 31);
+      const uint32_t v = c < pw ? (uint32_t)s_img[r][c] * s_img[r][c] : 0u;
+      uint32_t incl = v;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if ((int)(threadIdx.x & 31) >= d) incl += o;
+      }
+      if (c < pw) s_sq[r][c + 1] = carry + incl;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if ((threadIdx.x & 31) == 0) s_sq[r][0] = 0;
+  }
+  __syncthreads();
+  const unsigned long long tss = s_tss;
+  unsigned long long mykey = ~0ull;
+  // work items: (row r, group of 4 positions starting at 4 gq)
+  const uint32_t groups = (rc.w + 3) / 4;
+  for (uint32_t it = threadIdx.x; it < rc.h * groups; it += blockDim.x) {
+    const uint32_t r = it / groups, x4 = 4 * (it % groups);
+    uint32_t X[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
+    for (uint32_t dy = 0; dy < (uint32_t)kTpl; ++dy) {
+      const uint32_t* row = reinterpret_cast<const uint32_t*>(&s_img[r + dy][0]) + (x4 >> 2);
+      const uint32_t* trow = &s_tpl[dy][0];
+      uint32_t cur = row[0];
+#pragma unroll
+      for (int k2 = 0; k2 < kTpl / 4; ++k2) {
+        const uint32_t nxt = row[k2 + 1];
+        const uint32_t tw = trow[k2];
+        X[0] = __dp4a(cur, tw, X[0]);
+        X[1] = __dp4a(__byte_perm(cur, nxt, 0x4321), tw, X[1]);
+        X[2] = __dp4a(__byte_perm(cur, nxt, 0x5432), tw, X[2]);
+        X[3] = __dp4a(__byte_perm(cur, nxt, 0x6543), tw, X[3]);
+        cur = nxt;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const uint32_t xl = x4 + s;
+      if (xl >= rc.w) break;
+      unsigned long long Y = 0ull;
+      for (uint32_t dy = 0; dy < (uint32_t)kTpl; ++dy) Y += s_sq[r + dy][xl + kTpl] - s_sq[r + dy][xl];
+      const unsigned long long sse = Y + tss - 2ull * X[s];
+      const float score = (float)sse;  // round to nearest
+      const uint32_t idx = (rc.y0 + r) * Wo + rc.x0 + xl;
+      const unsigned long long key = ((unsigned long long)okey(score) << 32) | idx;
+      mykey = key < mykey ? key : mykey;
+    }
+  }
+  for (int d = 16; d; d >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, mykey, d);
+    mykey = o < mykey ? o : mykey;
+  }
+  if ((threadIdx.x & 31) == 0) s_best[threadIdx.x >> 5] = mykey;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long b = s_best[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) b = s_best[i] < b ? s_best[i] : b;
+    atomicMin(best + t, b);
+  }
+  (void)H;
+}
+
+// rectangles of the top-k windows: 32 x 32 positions centred on each
+// proposal's full-resolution estimate 4 (p - 5) + 2, moved inside the map
+__global__ void windows_kernel(const TopK* __restrict__ tk, uint32_t T, uint32_t Ws, uint32_t Wo, uint32_t Ho,
+                               Rect* __restrict__ rects, uint32_t* __restrict__ counts, uint32_t max_rects,
+                               unsigned long long* __restrict__ best) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const TopK& r = tk[t];
+  const uint32_t ww = Wo < (uint32_t)kWin ? Wo : kWin, wh = Ho < (uint32_t)kWin ? Ho : kWin;
+  for (uint32_t i = 0; i < r.count; ++i) {
+    const int px = (int)(r.pos[i] % Ws), py = (int)(r.pos[i] / Ws);
+    int cx = 4 * (px - kCentre) + 2 - kWin / 2, cy = 4 * (py - kCentre) + 2 - kWin / 2;
+    cx = cx < 0 ? 0 : (cx > (int)(Wo - ww) ? (int)(Wo - ww) : cx);
+    cy = cy < 0 ? 0 : (cy > (int)(Ho - wh) ? (int)(Ho - wh) : cy);
+    rects[(size_t)t * max_rects + i] = Rect{(uint32_t)cx, (uint32_t)cy, ww, wh};
+  }
+  counts[t] = r.count;
+  best[t] = ~0ull;
+}
+
+// ---- 4. certification tables ----------------------------------------------------------
+// Fine table: for each block (bx, by) of 12 x 12 box-sum origins q (q from 0
+// to W - 12, H - 12), the minimum and maximum of the 12 x 12 box sum B(q).
+// One block of threads per 4 x 4 fine blocks (48 x 48 origins).
+__global__ void __launch_bounds__(256) fine_table_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
+                                                         uint32_t Fx, uint32_t Fy, uint2* __restrict__ fine) {
+  __shared__ uint8_t s_img[48 + kBlk - 1][48 + kBlk - 1 + 1];
+  __shared__ uint32_t s_row[48 + kBlk - 1][48];
+  __shared__ uint32_t s_mn[16], s_mx[16];
+  const uint32_t qx0 = blockIdx.x * 48, qy0 = blockIdx.y * 48;
+  const uint32_t Qx = W - kBlk + 1, Qy = H - kBlk + 1;  // box-sum origins
+  for (uint32_t i = threadIdx.x; i < 59 * 59; i += blockDim.x) {
+    const uint32_t r = i / 59, c = i % 59, y = qy0 + r, x = qx0 + c;
+    s_img[r][c] = (y < H && x < W) ? img[(size_t)y * W + x] : 0;
+  }
+  if (threadIdx.x < 16) {
+    s_mn[threadIdx.x] = 0xFFFFFFFFu;
+    s_mx[threadIdx.x] = 0u;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 59 * 48; i += blockDim.x) {
+    const uint32_t r = i / 48, c = i % 48;
+    uint32_t s = 0;
+#pragma unroll
+    for (int d = 0; d < kBlk; ++d) s += s_img[r][c + d];
+    s_row[r][c] = s;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < 48 * 48; i += blockDim.x) {
+    const uint32_t r = i / 48, c = i % 48;
+    if (qy0 + r >= Qy || qx0 + c >= Qx) continue;
+    uint32_t s = 0;
+#pragma unroll
+    for (int d = 0; d < kBlk; ++d) s += s_row[r + d][c];
+    const uint32_t b = (r / kBlk) * 4 + c / kBlk;
+    atomicMin(&s_mn[b], s);
+    atomicMax(&s_mx[b], s);
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    const uint32_t bx = blockIdx.x * 4 + (threadIdx.x & 3), by = blockIdx.y * 4 + (threadIdx.x >> 2);
+    if (bx < Fx && by < Fy) fine[(size_t)by * Fx + bx] = make_uint2(s_mn[threadIdx.x], s_mx[threadIdx.x]);
+  }
+}
+
+// Coarse table: min / max of the fine table over the 4 x 4 fine blocks
+// starting at each fine block (clipped at the edges).
+__global__ void coarse_table_kernel(const uint2* __restrict__ fine, uint32_t Fx, uint32_t Fy,
+                                    uint2* __restrict__ coarse) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Fx * Fy) return;
+  const uint32_t bx = i % Fx, by = i / Fx;
+  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+  for (uint32_t dy = 0; dy < 4 && by + dy < Fy; ++dy)
+    for (uint32_t dx = 0; dx < 4 && bx + dx < Fx; ++dx) {
+      const uint2 v = fine[(size_t)(by + dy) * Fx + bx + dx];
+      mn = v.x < mn ? v.x : mn;
+      mx = v.y > mx ? v.y : mx;
+    }
+  coarse[i] = make_uint2(mn, mx);
+}
+
+// ---- 4b. certification of one template (one block per template) ---------------------------
+// status: 0 certified (extra rectangles, if any, still to verify), 1 low
+// margin, 2 too many uncertified blocks
+__device__ __forceinline__ unsigned long long lb_term(uint32_t st, uint2 mm) {
+  const uint32_t d = st < mm.x ? mm.x - st : (st > mm.y ? st - mm.y : 0u);
+  return (unsigned long long)d * d;
+}
+
+__global__ void __launch_bounds__(1024) certify_kernel(const uint8_t* __restrict__ tpl, const TopK* __restrict__ tk,
+                                                       float min_margin, const unsigned long long* __restrict__ best,
+                                                       const uint2* __restrict__ fine, const uint2* __restrict__ coarse,
+                                                       uint32_t Fx, uint32_t Fy, uint32_t Wo, uint32_t Ho,
+                                                       const Rect* __restrict__ wins, const uint32_t* __restrict__ nwin,
+                                                       uint32_t max_rects, Rect* __restrict__ extra,
+                                                       uint32_t* __restrict__ n_extra, uint32_t* __restrict__ status) {
+  __shared__ uint32_t s_st[16];
+  __shared__ Rect s_win[kMaxTopK];
+  __shared__ uint32_t s_count;
+  const uint32_t t = blockIdx.x;
+  if (tk[t].margin < min_margin || tk[t].count == 0) {
+    if (threadIdx.x == 0) {
+      status[t] = 1;
+      n_extra[t] = 0;
+    }
+    return;
+  }
+  const uint8_t* tp = tpl + (size_t)t * kTpl * kTpl;
+  if (threadIdx.x < 16) {
+    const uint32_t by = threadIdx.x >> 2, bx = threadIdx.x & 3;
+    uint32_t s = 0;
+    for (int dy = 0; dy < kBlk; ++dy)
+      for (int dx = 0; dx < kBlk; ++dx) s += tp[(by * kBlk + dy) * kTpl + bx * kBlk + dx];
+    s_st[threadIdx.x] = s;
+  }
+  const uint32_t nw = nwin[t];
+  if (threadIdx.x < nw) s_win[threadIdx.x] = wins[(size_t)t * max_rects + threadIdx.x];
+  if (threadIdx.x == 0) s_count = 0;
+  __syncthreads();
+  // the verified minimum; a block is excluded when RN_f32(ceil(LB)) > it
+  const float sstar = okey_value((uint32_t)(best[t] >> 32));
+  const uint32_t Px = (Wo + kBlk - 1) / kBlk, Py = (Ho + kBlk - 1) / kBlk;  // position blocks
+  const uint32_t Cqx = (Px + 3) / 4, Cqy = (Py + 3) / 4;
+  auto excluded = [&](unsigned long long num) {
+    const unsigned long long lb = (num + 143ull) / 144ull;  // SSE is an integer >= num / 144
+    return (float)lb > sstar;
+  };
+  for (uint32_t q = threadIdx.x; q < Cqx * Cqy; q += blockDim.x) {
+    const uint32_t qx = q % Cqx, qy = q / Cqx;
+    unsigned long long num = 0ull;
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+      const uint32_t fx = 4 * qx + (b & 3), fy = 4 * qy + (b >> 2);
+      if (fx < Fx && fy < Fy) num += lb_term(s_st[b], coarse[(size_t)fy * Fx + fx]);
+    }
+    if (excluded(num)) continue;
+    for (uint32_t k = 0; k < 16; ++k) {
+      const uint32_t bx = 4 * qx + (k & 3), by = 4 * qy + (k >> 2);
+      if (bx >= Px || by >= Py) continue;
+      unsigned long long n2 = 0ull;
+#pragma unroll
+      for (int b = 0; b < 16; ++b) {
+        const uint32_t fx = bx + (b & 3), fy = by + (b >> 2);
+        if (fx < Fx && fy < Fy) n2 += lb_term(s_st[b], fine[(size_t)fy * Fx + fx]);
+      }
+      if (excluded(n2)) continue;
+      const uint32_t x0 = bx * kBlk, y0 = by * kBlk;
+      const uint32_t x1 = min(x0 + kBlk, Wo), y1 = min(y0 + kBlk, Ho);
+      bool covered = false;
+      for (uint32_t w = 0; w < nw && !covered; ++w) {
+        const Rect r = s_win[w];
+        covered = x0 >= r.x0 && y0 >= r.y0 && x1 <= r.x0 + r.w && y1 <= r.y0 + r.h;
+      }
+      if (covered) continue;
+      const uint32_t slot = atomicAdd(&s_count, 1u);
+      if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = Rect{x0, y0, x1 - x0, y1 - y0};
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t c = s_count;
+    status[t] = c > kMaxExtra ? 2u : 0u;
+    n_extra[t] = c > kMaxExtra ? 0u : c;
+  }
+}
+
+}  // namespace
+}  // namespace learned
+}  // namespace ipb
+
+// ============================================================================
+// C ABI
+// ============================================================================
+using namespace ipb;
+using namespace ipb::learned;
+
+struct ipb_proposal_net;  // tm_learned.cu
+namespace ipb {
+namespace learned {
+// network accessors (tm_learned.cu)
+const PackedWeights& net_weights(const ipb_proposal_net* net);
+}  // namespace learned
+}  // namespace ipb
+
+namespace {
+
+ipb_status pfail(ipb_status st, const std::string& msg) {
+  report_error(st, msg.c_str());
+  return st;
+}
+ipb_status pcuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return IPB_OK;
+  (void)cudaGetLastError();
+  return pfail(e == cudaErrorMemoryAllocation ? IPB_ERR_OUT_OF_MEMORY : IPB_ERR_CUDA,
+               std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define P_CUDA(call, what)                      \
+  do {                                          \
+    const ipb_status st_ = pcuda((call), what); \
+    if (st_ != IPB_OK) return st_;              \
+  } while (0)
+
+struct ProposeScratch {
+  int device = -1;
+  void* p = nullptr;
+  size_t bytes = 0;
+  unsigned int* err = nullptr;
+  unsigned int tag = 0;
+  ~ProposeScratch() {
+    if (device >= 0) {
+      cudaSetDevice(device);
+      cudaDeviceSynchronize();
+      if (p) cudaFree(p);
+      if (err) cudaFree(err);
+    }
+  }
+};
+
+struct Carve {
+  uint4* a;
+  uint4* b;
+  uint4* F;
+  uint4* ta;
+  uint4* tb;
+  uint4* Ft;
+  float* G;
+  uint16_t* gb;
+  unsigned long long* cells;
+  TopK* tk;
+  Rect* wins;
+  uint32_t* nwin;
+  Rect* extra;
+  uint32_t* n_extra;
+  uint32_t* status;
+  unsigned long long* best;
+  uint2* fine;
+  uint2* coarse;
+  uint8_t* fb_tpl;
+  unsigned long long* fb_keys;
+  ipb_extremes_f32* fb_ext;
+  size_t bytes;
+};
+
+Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
+  Carve c{};
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    uint8_t* p = base ? base + off : nullptr;
+    off += align_up(b ? b : 1, 256);
+    return p;
+  };
+  const uint32_t Hs = H / 4, Ws = W / 4;
+  const size_t su = act_units(1, Hs, Ws) * 16, tu = act_units(T, kTplDs, kTplDs) * 16;
+  c.a = reinterpret_cast<uint4*>(take(su));
+  c.b = reinterpret_cast<uint4*>(take(su));
+  c.F = reinterpret_cast<uint4*>(take(su));
+  c.ta = reinterpret_cast<uint4*>(take(tu));
+  c.tb = reinterpret_cast<uint4*>(take(tu));
+  c.Ft = reinterpret_cast<uint4*>(take(tu));
+  c.G = reinterpret_cast<float*>(take((size_t)T * kEmb * 4));
+  c.gb = reinterpret_cast<uint16_t*>(take((size_t)T * kEmb * 2));
+  const uint32_t Cx = (Ws + kCell - 1) / kCell, Cy = (Hs + kCell - 1) / kCell;
+  c.cells = reinterpret_cast<unsigned long long*>(take((size_t)T * Cx * Cy * 8));
+  c.tk = reinterpret_cast<TopK*>(take((size_t)T * sizeof(TopK)));
+  c.wins = reinterpret_cast<Rect*>(take((size_t)T * k * sizeof(Rect)));
+  c.nwin = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
+  c.extra = reinterpret_cast<Rect*>(take((size_t)T * kMaxExtra * sizeof(Rect)));
+  c.n_extra = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
+  c.status = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
+  c.best = reinterpret_cast<unsigned long long*>(take((size_t)T * 8));
+  const uint32_t Fx = (W - kBlk + 1 + kBlk - 1) / kBlk, Fy = (H - kBlk + 1 + kBlk - 1) / kBlk;
+  c.fine = reinterpret_cast<uint2*>(take((size_t)Fx * Fy * 8));
+  c.coarse = reinterpret_cast<uint2*>(take((size_t)Fx * Fy * 8));
+  c.fb_tpl = reinterpret_cast<uint8_t*>(take((size_t)T * kTpl * kTpl));
+  c.fb_keys = reinterpret_cast<unsigned long long*>(take((size_t)T * 16));
+  c.fb_ext = reinterpret_cast<ipb_extremes_f32*>(take((size_t)T * sizeof(ipb_extremes_f32)));
+  c.bytes = off;
+  return c;
+}
+
+ProposeScratch& scratch_for_thread() {
+  thread_local ProposeScratch s;
+  return s;
+}
+
+}  // namespace
+
+IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, const uint8_t* d_image,
+                                                uint32_t image_width, uint32_t image_height,
+                                                const uint8_t* d_templates, uint32_t template_width,
+                                                uint32_t template_height, uint32_t n_templates, int method,
+                                                const ipb_propose_options* options, ipb_proposal_result* results,
+                                                void* stream) {
+  const uint32_t W = image_width, H = image_height, T = n_templates;
+  if (!net || !d_image || !d_templates || !results) return pfail(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (template_width != (uint32_t)kTpl || template_height != (uint32_t)kTpl)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, "the proposal network takes 48 x 48 templates");
+  if (method != IPB_SUM_OF_SQUARED_ERRORS)
+    return pfail(IPB_ERR_INVALID_ARGUMENT,
+                 "learned proposals answer SumOfSquaredErrors queries (their certificate bounds that score)");
+  if (W % 32 || H % 32 || W < 64 || H < 64)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, "learned proposals take images whose sides are multiples of 32 (>= 64)");
+  if (T == 0) return IPB_OK;
+  ipb_propose_options opt{16u, 0.1f, 1};
+  if (options) opt = *options;
+  if (opt.top_k == 0 || opt.top_k > (uint32_t)kMaxTopK)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, "top_k must be 1..32");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ProposeScratch& ps = scratch_for_thread();
+  int dev = 0;
+  P_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  const Carve need = carve(nullptr, W, H, T, opt.top_k);
+  if (ps.device != dev || ps.bytes < need.bytes) {
+    if (ps.p) {
+      P_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+      cudaFree(ps.p);
+      ps.p = nullptr;
+      ps.bytes = 0;
+    }
+    if (ps.err && ps.device != dev) {
+      cudaFree(ps.err);
+      ps.err = nullptr;
+    }
+    ps.device = dev;
+    P_CUDA(cudaMalloc(&ps.p, need.bytes), "cudaMalloc (proposal scratch)");
+    ps.bytes = need.bytes;
+    if (!ps.err) {
+      P_CUDA(cudaMalloc(&ps.err, sizeof(unsigned int)), "cudaMalloc");
+      P_CUDA(cudaMemset(ps.err, 0, sizeof(unsigned int)), "cudaMemset");
+    }
+  }
+  const Carve c = carve(static_cast<uint8_t*>(ps.p), W, H, T, opt.top_k);
+  const PackedWeights& pw = net_weights(net);
+  const uint32_t Hs = H / 4, Ws = W / 4, Wo = W - kTpl + 1, Ho = H - kTpl + 1;
+  const uint32_t Cx = Ws / kCell, Cy = Hs / kCell;
+  const uint32_t Fx = (W - kBlk + 1 + kBlk - 1) / kBlk, Fy = (H - kBlk + 1 + kBlk - 1) / kBlk;
+
+  // 1. trunk of the image and of the templates, embedding, heatmap cells
+  P_CUDA(launch_trunk(d_image, 1, H, W, pw, nullptr, c.a, c.b, c.F, s), "image trunk");
+  P_CUDA(launch_trunk(d_templates, T, kTpl, kTpl, pw, nullptr, c.ta, c.tb, c.Ft, s), "template trunk");
+  P_CUDA(launch_embed(c.Ft, T, c.G, s), "embedding");
+  pack_embedding_kernel<<<(T * kEmb + 255) / 256, 256, 0, s>>>(c.G, T, c.gb);
+  count_launch(kKernelPropose);
+  const dim3 hg((Ws + kHW - 1) / kHW, Hs / kCell, (T + 31) / 32);
+  head_cells_kernel<<<hg, 256, 0, s>>>(c.F, Hs, Ws, c.gb, T, c.cells);
+  count_launch(kKernelPropose);
+  P_CUDA(cudaGetLastError(), "heatmap");
+  // 2. top-k and margins
+  topk_kernel<<<T, 1024, 0, s>>>(c.cells, Cy, Cx, Ws, opt.top_k, c.tk);
+  count_launch(kKernelPropose);
+  // 3. windows and their exact scores
+  windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(c.tk, T, Ws, Wo, Ho, c.wins, c.nwin, opt.top_k, c.best);
+  count_launch(kKernelPropose);
+  verify_kernel<<<dim3(opt.top_k, T), 256, 0, s>>>(d_image, W, H, d_templates, c.wins, c.nwin, opt.top_k, c.best);
+  count_launch(kKernelPropose);
+  P_CUDA(cudaGetLastError(), "verification");
+  // 4. certification
+  if (opt.certify) {
+    fine_table_kernel<<<dim3((Fx + 3) / 4, (Fy + 3) / 4), 256, 0, s>>>(d_image, W, H, Fx, Fy, c.fine);
+    count_launch(kKernelPropose);
+    coarse_table_kernel<<<(Fx * Fy + 255) / 256, 256, 0, s>>>(c.fine, Fx, Fy, c.coarse);
+    count_launch(kKernelPropose);
+    certify_kernel<<<T, 1024, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.fine, c.coarse, Fx, Fy, Wo, Ho,
+                                      c.wins, c.nwin, opt.top_k, c.extra, c.n_extra, c.status);
+    count_launch(kKernelPropose);
+    verify_kernel<<<dim3(kMaxExtra, T), 256, 0, s>>>(d_image, W, H, d_templates, c.extra, c.n_extra, kMaxExtra,
+                                                     c.best);
+    count_launch(kKernelPropose);
+    P_CUDA(cudaGetLastError(), "certification");
+  }
+  // 5. the verdicts to the host; fallback templates through the exhaustive kernel
+  std::vector<TopK> tk(T);
+  std::vector<uint32_t> status(T, 0u);
+  std::vector<unsigned long long> best(T);
+  P_CUDA(cudaMemcpyAsync(tk.data(), c.tk, sizeof(TopK) * T, cudaMemcpyDeviceToHost, s), "copy proposals");
+  P_CUDA(cudaMemcpyAsync(best.data(), c.best, sizeof(unsigned long long) * T, cudaMemcpyDeviceToHost, s),
+         "copy scores");
+  if (opt.certify)
+    P_CUDA(cudaMemcpyAsync(status.data(), c.status, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s), "copy status");
+  P_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  std::vector<uint32_t> fb;
+  for (uint32_t t = 0; t < T; ++t) {
+    if (!opt.certify && (tk[t].margin < opt.min_margin || tk[t].count == 0)) status[t] = 1;
+    if (status[t]) fb.push_back(t);
+  }
+  std::vector<ipb_extremes_f32> fb_ext(fb.size());
+  if (!fb.empty()) {
+    for (size_t i = 0; i < fb.size(); ++i)
+      P_CUDA(cudaMemcpyAsync(c.fb_tpl + i * kTpl * kTpl, d_templates + (size_t)fb[i] * kTpl * kTpl, kTpl * kTpl,
+                             cudaMemcpyDeviceToDevice, s),
+             "gather fallback templates");
+    const uint32_t nf = (uint32_t)fb.size();
+    P_CUDA(launch_many_keys_init(c.fb_keys, nf, s), "extremes init");
+    ps.tag += 1;
+    P_CUDA(launch_many(d_image, W, H, c.fb_tpl, kTpl, kTpl, nf, IPB_SUM_OF_SQUARED_ERRORS,
+                       IPB_PRECISION_EXACT_FP64, nullptr, c.fb_keys, ps.err, ps.tag, s, nullptr),
+           "exhaustive fallback");
+    P_CUDA(launch_many_keys_finish(c.fb_keys, Wo, c.fb_ext, nf, s), "extremes finish");
+    unsigned int failed = 0;
+    P_CUDA(cudaMemcpyAsync(fb_ext.data(), c.fb_ext, sizeof(ipb_extremes_f32) * nf, cudaMemcpyDeviceToHost, s),
+           "copy fallback results");
+    P_CUDA(cudaMemcpyAsync(&failed, ps.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "copy error word");
+    P_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (failed >= ps.tag)
+      return pfail(IPB_ERR_TIMEOUT, "the exhaustive fallback kernel timed out waiting on its pipeline");
+  }
+  size_t f = 0;
+  for (uint32_t t = 0; t < T; ++t) {
+    ipb_proposal_result& r = results[t];
+    r.margin = tk[t].margin;
+    r.path = status[t];
+    if (status[t]) {
+      const ipb_extremes_f32& e = fb_ext[f++];
+      r.value = e.min_value;
+      r.x = e.min_value_location_x;
+      r.y = e.min_value_location_y;
+    } else {
+      const unsigned long long k = best[t];
+      r.value = okey_value((uint32_t)(k >> 32));
+      const uint32_t idx = (uint32_t)(k & 0xFFFFFFFFu);
+      r.x = idx % Wo;
+      r.y = idx / Wo;
+    }
+  }
+  return IPB_OK;
+}

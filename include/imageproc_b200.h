@@ -321,6 +321,78 @@ ipb_status ipb_match_templates_device(const uint8_t *d_image, uint32_t image_wid
                                       float *d_out, ipb_extremes_f32 *d_extremes,
                                       void *stream);
 
+/* ---- learned proposals -------------------------------------------------------
+ * Additive API with no counterpart in the reference, which scores every
+ * window. For many 48 x 48 templates against one large image, a small
+ * convolutional network (bf16 weights, fp32 accumulation) proposes windows;
+ * their scores are computed exactly, a lower bound on every other window
+ * certifies the answer, and templates that cannot be certified (or whose
+ * heatmap margin is low) are answered by the exhaustive kernel. The answer
+ * is what match_template (src/template_matching.rs:78-92) followed by
+ * find_extremes (:479-511) gives for SumOfSquaredErrors: the first minimum in
+ * row-major order of the EXACT_FP64 score map.
+ *
+ * The network: 4 x 4 box downsample, five 3 x 3 convolutions of 32 channels
+ * (ReLU after the first four), and a 2 x 2 x 32 embedding of each template
+ * (the same layers applied to the template) correlated with the image's
+ * features. Parameters are IPB_PROPOSAL_NET_PARAMS fp32 values:
+ * W1 [32][1][3][3], b1 [32], then W2..W5 [32][32][3][3] each followed by its
+ * bias [32]. */
+#define IPB_PROPOSAL_NET_PARAMS 37312
+typedef struct ipb_proposal_net ipb_proposal_net;
+
+/* A network on the current device with the given parameters (host array). */
+ipb_status ipb_proposal_net_create(const float *params, ipb_proposal_net **net);
+ipb_status ipb_proposal_net_destroy(ipb_proposal_net *net);
+/* The current parameters (host array of IPB_PROPOSAL_NET_PARAMS floats). */
+ipb_status ipb_proposal_net_get_params(const ipb_proposal_net *net, float *params);
+
+/* Training. A batch is n_scenes crops of scene_height x scene_width u8
+ * (sides multiples of 4) and n_templates (<= 128) 48 x 48 templates, all on
+ * the device, back to back. d_positives (device, int64, one per template)
+ * holds each template's target heatmap position as a flat index into the
+ * crops' downsampled positions: (crop * (scene_height / 4) + py) *
+ * (scene_width / 4) + px, where (px, py) = the downsampled position of the
+ * template's best window (from the exhaustive kernel) plus 5. The loss is the
+ * softmax cross-entropy of each template's logits over all positions of all
+ * crops. _gradients writes the loss and the gradients (host, same layout as
+ * the parameters); _train_step takes one Adam step (beta 0.9, 0.999). */
+ipb_status ipb_proposal_net_gradients(ipb_proposal_net *net, const uint8_t *d_scenes, uint32_t n_scenes,
+                                      uint32_t scene_height, uint32_t scene_width,
+                                      const uint8_t *d_templates, uint32_t n_templates,
+                                      const int64_t *d_positives, float *h_loss, float *h_grads,
+                                      void *stream);
+ipb_status ipb_proposal_net_train_step(ipb_proposal_net *net, const uint8_t *d_scenes, uint32_t n_scenes,
+                                       uint32_t scene_height, uint32_t scene_width,
+                                       const uint8_t *d_templates, uint32_t n_templates,
+                                       const int64_t *d_positives, float learning_rate, float *h_loss,
+                                       void *stream);
+
+typedef struct ipb_propose_options {
+    uint32_t top_k;    /* windows of 32 x 32 positions verified per template (1..32, default 16) */
+    float min_margin;  /* heatmap confidence margin below which a template falls back (default 0.1) */
+    int certify;       /* 1 (default): certify answers; 0: accept the verified windows' best */
+} ipb_propose_options;
+
+typedef struct ipb_proposal_result {
+    float value;        /* the minimum SumOfSquaredErrors score */
+    uint32_t x, y;      /* its first location in row-major order */
+    float margin;       /* the heatmap's confidence margin */
+    uint32_t path;      /* 0: proposals, verified and certified; 1: fallback (low margin);
+                           2: fallback (not certified) */
+} ipb_proposal_result;
+
+/* Answers n_templates SumOfSquaredErrors queries of 48 x 48 templates
+ * (device, back to back) against one image (device; sides multiples of 32)
+ * and writes one result per template to `results` (host). options may be
+ * NULL (defaults). Synchronises `stream` before returning. */
+ipb_status ipb_propose_and_match_device(const ipb_proposal_net *net, const uint8_t *d_image,
+                                        uint32_t image_width, uint32_t image_height,
+                                        const uint8_t *d_templates, uint32_t template_width,
+                                        uint32_t template_height, uint32_t n_templates, int method,
+                                        const ipb_propose_options *options, ipb_proposal_result *results,
+                                        void *stream);
+
 /* ---- find_extremes -------------------------------------------------------- */
 
 /* Extremes<T> (src/template_matching.rs:463-475), field order kept. */

@@ -322,3 +322,64 @@ def template_matching_example(image, x, y, w, h, precision=0) -> dict:
         padded[h // 2:h // 2 + scaled.shape[0], w // 2:w // 2 + scaled.shape[1]] = scaled
         out[name] = draw_green_rect(padded, x, y, w, h)
     return out
+
+
+# ---- the proposal network (learned_oracle.c) ------------------------------------
+
+class _LoParams(C.Structure):
+    _fields_ = [("W", C.c_void_p * 5), ("b", C.c_void_p * 5), ("alpha", C.c_double)]
+
+
+class _LoGrads(C.Structure):
+    _fields_ = [("dW", C.c_void_p * 5), ("db", C.c_void_p * 5)]
+
+
+_LO_SHAPES = [(32, 1, 3, 3)] + [(32, 32, 3, 3)] * 4
+
+
+def _lo_split(params):
+    """Parameter vector (the library's layout) -> lists of FP64 weights and biases."""
+    p = np.asarray(params, np.float64)
+    Ws, bs, off = [], [], 0
+    for shp in _LO_SHAPES:
+        n = int(np.prod(shp))
+        Ws.append(np.ascontiguousarray(p[off:off + n].reshape(shp)))
+        off += n
+        bs.append(np.ascontiguousarray(p[off:off + 32]))
+        off += 32
+    assert off == p.size
+    return Ws, bs
+
+
+def learned_loss_grad(params, scenes, templates, positives, bf16=True, alpha=0.125, want_logits=False):
+    """FP64 loss and gradients of the proposal network (learned_oracle.c):
+    scenes (n, h, w) u8, templates (t, 48, 48) u8, positives (t,) flat indices.
+    Returns (loss, grads in the parameter layout[, logits (t, n*h/4*w/4)])."""
+    L = lib()
+    if not getattr(L, "_lo_bound", False):
+        L.lo_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.lo_loss_grad.restype = C.c_double
+        L._lo_bound = True
+    scenes = np.ascontiguousarray(scenes, np.uint8)
+    templates = np.ascontiguousarray(templates, np.uint8)
+    pos = np.ascontiguousarray(positives, np.int64)
+    n, h, w = scenes.shape
+    t = templates.shape[0]
+    Ws, bs = _lo_split(params)
+    P = _LoParams()
+    for k in range(5):
+        P.W[k] = Ws[k].ctypes.data
+        P.b[k] = bs[k].ctypes.data
+    P.alpha = alpha
+    dW = [np.zeros_like(x) for x in Ws]
+    db = [np.zeros_like(x) for x in bs]
+    G = _LoGrads()
+    for k in range(5):
+        G.dW[k] = dW[k].ctypes.data
+        G.db[k] = db[k].ctypes.data
+    z = np.empty((t, n * (h // 4) * (w // 4)), np.float64) if want_logits else None
+    loss = L.lo_loss_grad(C.byref(P), _p(scenes), n, h, w, _p(templates), t, _p(pos), int(bf16), C.byref(G),
+                          _p(z))
+    grads = np.concatenate([np.concatenate([dW[k].reshape(-1), db[k]]) for k in range(5)])
+    return (loss, grads, z) if want_logits else (loss, grads)
