@@ -665,10 +665,11 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl)
   return false;
 }
 
-// Template shapes the tensor path takes: at least one K step of 16 bytes and
+// Template shapes the tensor path takes: at least 8 columns (templates of
+// 8..15 columns fill half of the first 32-byte K step, zeros the rest) and
 // one 8-row band; rows within the band table; s32 sums exact (33025 pixels).
 bool umma_shape_ok(uint32_t w, uint32_t h, bool masked) {
-  return w >= 16 && h >= 8 && h <= 128 && w <= (masked ? 128u : 256u) && (size_t)w * h <= 33025;
+  return w >= 8 && h >= 8 && h <= 128 && w <= (masked ? 128u : 256u) && (size_t)w * h <= 33025;
 }
 
 }  // namespace

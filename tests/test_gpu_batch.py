@@ -22,7 +22,7 @@ def bits(a):
 
 def _mixed_items(seed, n):
     """Uneven pairs: tensor-core shapes of every row width, CUDA-core shapes
-    (templates narrower than 16 or general masks), binary masks, all methods."""
+    (templates narrower than 8 or general masks), binary masks, all methods."""
     g = np.random.default_rng(seed)
     items = []
     for k in range(n):

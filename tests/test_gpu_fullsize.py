@@ -6,7 +6,7 @@
   Every pair's fused extremes must equal the oracle's find_extremes of the
   oracle's map (src/template_matching.rs:479-511, first occurrence), and the
   full maps of at least 16 pairs (the largest image, the largest template,
-  every method, both kernel families, seeded picks) must equal the oracle's
+  every method, the narrowest templates, seeded picks) must equal the oracle's
   bit for bit (match_template, :78-92).
 * Many templates: the 4096 x 4096 value-noise scene with its 512 templates of
   32 x 32 (synthetic.value_noise_scene(), the benchmark's draw),
@@ -52,10 +52,10 @@ def _full_map_picks(pairs, n_picks=16, seed=17):
     picks = {int(np.argmax(area)), int(np.argmax(tarea))}
     for m in range(4):  # every method
         picks.add(next(k for k, p in enumerate(pairs) if p[2] == m))
-    # both kernel families: the tensor path takes templates of >= 16 columns and
-    # >= 8 rows (these draws are all >= 8 rows), the CUDA-core kernel the rest
+    # the narrowest templates (8..15 columns: half of the first 32-byte K step
+    # of the tensor-core kernel) and a wide one
     picks.add(next(k for k, (_, t, _) in enumerate(pairs) if t.shape[1] < 16))
-    picks.add(next(k for k, (_, t, _) in enumerate(pairs) if t.shape[1] >= 16))
+    picks.add(next(k for k, (_, t, _) in enumerate(pairs) if t.shape[1] >= 64))
     g = np.random.default_rng(seed)
     for k in g.permutation(len(pairs)):
         if len(picks) >= n_picks:
@@ -75,7 +75,7 @@ def test_uneven_pairs_full_draw():
     batch = device.Batch(items, extremes=True)
     plan = device.BatchPlan(batch, tm.Precision.ExactFp64)
     info = plan.info()
-    assert 0 < info["tensor_pairs"] < 256  # both kernel families are in the draw
+    assert info["tensor_pairs"] > 0
     plan.launch()
     torch.cuda.synchronize()
     got_ext = [_ext_tuple(e) for e in batch.extremes_host()]

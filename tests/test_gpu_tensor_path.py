@@ -45,6 +45,8 @@ SHAPES = [
     ((400, 600), (100, 256)),   # 256-byte rows, 64-row tiles
     ((130, 130), (8, 17)),      # short template
     ((64, 300), (64, 20)),      # one output row band
+    ((150, 333), (12, 9)),      # narrow template: half of the first K step
+    ((97, 260), (8, 8)),        # the narrowest and shortest template taken
 ]
 
 

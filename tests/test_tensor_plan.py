@@ -25,13 +25,13 @@ BAND_TABLE_OFFSET = 1024
 
 
 def shape_taken(w, h, masked):
-    return w >= 16 and 8 <= h <= 128 and w <= (128 if masked else 256) and w * h <= 33025
+    return w >= 8 and 8 <= h <= 128 and w <= (128 if masked else 256) and w * h <= 33025
 
 
 def shapes():
     for masked in (False, True):
         for h in range(8, 129):
-            for w in range(16, 257):
+            for w in range(8, 257):
                 if shape_taken(w, h, masked):
                     yield w, h, masked
 
@@ -69,7 +69,7 @@ def test_window_sums_fit_s32_for_every_taken_shape():
 
 
 def test_shapes_outside_the_tensor_path_have_no_plan():
-    for w, h, masked in [(15, 8, False), (16, 7, False), (16, 129, False), (257, 8, False),
+    for w, h, masked in [(7, 8, False), (7, 16, True), (16, 7, False), (16, 129, False), (257, 8, False),
                          (129, 8, True), (256, 130, False)]:
         assert _lib.tensor_plan(w, h, masked, batch=False) is None
 
