@@ -175,6 +175,8 @@ def lib() -> C.CDLL:
     L.ipb_tensor_plan_for.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.POINTER(TensorPlan)]
     L.ipb_debug_set_pipeline_wait_ns.argtypes = [C.c_uint64]
     L.ipb_debug_set_pipeline_wait_ns.restype = None
+    L.ipb_debug_stall_pipelines.argtypes = [C.c_int]
+    L.ipb_debug_stall_pipelines.restype = None
     _lib = L
     return L
 

@@ -7,7 +7,9 @@
 // stream before touching scratch and records it afterwards, so calls from one
 // thread on different streams never overlap on shared scratch.
 #include <atomic>
+#include <condition_variable>
 #include <cstdio>
+#include <thread>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -107,6 +109,10 @@ std::atomic<unsigned long long> g_wait_ns{kDefaultWaitNs};
 }  // namespace
 
 unsigned long long pipeline_wait_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+namespace {
+std::atomic<bool> g_stall{false};
+}  // namespace
+bool pipeline_stall() { return g_stall.load(std::memory_order_relaxed); }
 
 int device_sm_count() {
   static std::atomic<int> cache[64] = {};
@@ -198,6 +204,11 @@ struct Context {
   cudaStream_t s_in = nullptr, s_out = nullptr;
   cudaStream_t s_band[kMaxBands] = {};
   cudaEvent_t band_in[kMaxBands] = {}, band_done[kMaxBands] = {}, out_done = nullptr;
+  // page-locked bounce buffer for pageable images of banded calls; free for
+  // reuse once stage_free (recorded after its last copy) has completed
+  void* stage = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_free = nullptr;
   ~Context() {
     if (device < 0) return;
     cudaSetDevice(device);
@@ -213,6 +224,11 @@ struct Context {
       if (band_done[b]) cudaEventDestroy(band_done[b]);
     }
     if (out_done) cudaEventDestroy(out_done);
+    if (stage_free) {
+      cudaEventSynchronize(stage_free);
+      cudaEventDestroy(stage_free);
+    }
+    if (stage) cudaFreeHost(stage);
     for (cudaStream_t s : {s_in, s_out})
       if (s) cudaStreamDestroy(s);
     for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys, &rgb, &keys})
@@ -381,6 +397,83 @@ ipb_status ensure_band_streams(Context* c, uint32_t nb) {
 // therefore run on streams of their own, each starting once its image rows
 // are in, beside the bands before it (they share no scratch). CUDA-core bands
 // share the context's scratch and run in order on the context's stream.
+// Host-to-host copies split over a few persistent threads (the calling
+// thread takes a share too). A pageable source cannot be read by the copy
+// engines directly: the driver would stage it through its own buffer at one
+// thread's memcpy rate while holding the calling thread. Copying it into a
+// page-locked buffer in parallel, band by band, lets each band's DMA start
+// while the next band's rows are still being copied.
+class CopyPool {
+ public:
+  static CopyPool& get() {
+    static CopyPool pool;
+    return pool;
+  }
+  void copy(uint8_t* dst, const uint8_t* src, size_t n) {
+    const size_t parts = n >= (size_t(1) << 19) ? workers_.size() + 1 : 1;
+    if (parts == 1) {
+      std::memcpy(dst, src, n);
+      return;
+    }
+    const size_t chunk = align_up((n + parts - 1) / parts, 4096);
+    std::unique_lock<std::mutex> lk(mu_);
+    size_t off = chunk;  // the caller copies [0, chunk)
+    for (; off < n; off += chunk) jobs_.push_back({dst + off, src + off, std::min(chunk, n - off)});
+    pending_ += jobs_.size();
+    lk.unlock();
+    cv_.notify_all();
+    std::memcpy(dst, src, std::min(chunk, n));
+    lk.lock();
+    done_.wait(lk, [&] { return pending_ == 0; });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (std::thread& t : workers_) t.join();
+  }
+
+ private:
+  struct Job {
+    uint8_t* dst;
+    const uint8_t* src;
+    size_t n;
+  };
+  CopyPool() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned n = hw >= 8 ? 3u : (hw >= 4 ? 1u : 0u);
+    for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { run(); });
+  }
+  void run() {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || !jobs_.empty(); });
+      if (stop_) return;
+      const Job j = jobs_.front();
+      jobs_.pop_front();
+      lk.unlock();
+      std::memcpy(j.dst, j.src, j.n);
+      lk.lock();
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  std::deque<Job> jobs_;
+  size_t pending_ = 0;
+  bool stop_ = false;
+  std::vector<std::thread> workers_;
+};
+
+bool host_memory_is_locked(const void* p) {
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, p) == cudaSuccess) return pa.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();  // not a pointer the runtime knows: pageable
+  return false;
+}
+
 ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* image, const uint8_t* tpl,
                              const uint8_t* mask, uint32_t nb, float* out) {
   ipb_status st;
@@ -392,13 +485,23 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
   // queued as soon as its launch is: they cross while the host still copies
   // later image rows from pageable memory (which holds the calling thread).
   // Into pageable memory the copy would hold the thread too: queued last.
-  cudaPointerAttributes pa{};
-  bool out_locked = false;
-  if (cudaPointerGetAttributes(&pa, out) == cudaSuccess)
-    out_locked = pa.type == cudaMemoryTypeHost;
-  else
-    (void)cudaGetLastError();  // not a pointer the runtime knows: pageable
+  const bool out_locked = host_memory_is_locked(out);
   const uint32_t W = full.W, Wo = full.W - full.w + 1, Ho = full.H - full.h + 1;
+  // a pageable image goes through the context's page-locked bounce buffer
+  const size_t ib = (size_t)W * full.H;
+  const bool staged = ib > 0 && !host_memory_is_locked(image);
+  if (staged) {
+    if (c->stage_free) IPB_CUDA(cudaEventSynchronize(c->stage_free), "cudaEventSynchronize");
+    if (c->stage_cap < ib) {
+      if (c->stage) cudaFreeHost(c->stage);
+      c->stage = nullptr;
+      c->stage_cap = 0;
+      IPB_CUDA(cudaMallocHost(&c->stage, align_up(ib, 1 << 20)), "cudaMallocHost (image staging)");
+      c->stage_cap = align_up(ib, 1 << 20);
+    }
+    if (!c->stage_free) IPB_CUDA(cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  const uint8_t* src_img = staged ? static_cast<const uint8_t*>(c->stage) : image;
   const size_t tb = (size_t)full.w * full.h;
   const uint32_t rows = (uint32_t)align_up((Ho + nb - 1) / nb, 16);
   uint8_t* d_img = static_cast<uint8_t*>(c->img.p);
@@ -417,7 +520,10 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
     uint32_t have = 0, bands = 0;  // image rows on the device, bands queued
     for (uint32_t o0 = 0; o0 < Ho; o0 += rows, ++bands) {
       const uint32_t o1 = std::min(Ho, o0 + rows), need = o1 + full.h - 1;
-      IPB_CUDA(cudaMemcpyAsync(d_img + (size_t)have * W, image + (size_t)have * W, (size_t)(need - have) * W,
+      if (staged)
+        CopyPool::get().copy(static_cast<uint8_t*>(c->stage) + (size_t)have * W, image + (size_t)have * W,
+                             (size_t)(need - have) * W);
+      IPB_CUDA(cudaMemcpyAsync(d_img + (size_t)have * W, src_img + (size_t)have * W, (size_t)(need - have) * W,
                                cudaMemcpyHostToDevice, c->s_in),
                "copy image rows");
       have = need;
@@ -446,6 +552,7 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
       IPB_CUDA(cudaEventRecord(c->band_done[bands], a.stream), "cudaEventRecord");
       if (out_locked && (st = queue_out(bands))) return st;
     }
+    if (staged) IPB_CUDA(cudaEventRecord(c->stage_free, c->s_in), "cudaEventRecord");
     if (!out_locked)
       for (uint32_t b = 0; b < bands; ++b)
         if ((st = queue_out(b))) return st;
@@ -662,6 +769,8 @@ IPB_API ipb_status ipb_set_precision(int precision) {
 }
 
 IPB_API int ipb_get_precision(void) { return g_precision.load(); }
+
+IPB_API void ipb_debug_stall_pipelines(int enable) { g_stall.store(enable != 0, std::memory_order_relaxed); }
 
 IPB_API void ipb_debug_set_pipeline_wait_ns(uint64_t ns) {
   g_wait_ns.store(ns ? (unsigned long long)ns : kDefaultWaitNs, std::memory_order_relaxed);

@@ -47,6 +47,10 @@ int device_sm_count();
 // Lowered only by the test entry point ipb_debug_set_pipeline_wait_ns.
 constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
 unsigned long long pipeline_wait_ns();
+// Failure-detection test hook: when set, the MMA warp of every tensor-core
+// kernel launched afterwards first waits on an mbarrier that nothing arrives
+// at, so that bounded wait runs out (ipb_debug_stall_pipelines).
+bool pipeline_stall();
 
 // ---- tracing ---------------------------------------------------------------
 // Every kernel launch site reports itself; the C ABI exposes the running
@@ -207,6 +211,7 @@ struct UmmaLaunch {
   unsigned int tag;
   // budget of the pipeline's bounded waits, per tile (pipeline_wait_ns())
   unsigned long long wait_ns;
+  uint32_t stall;  // pipeline_stall() at launch
   // {next tile counter, CTAs finished}, both zero at launch: tiles after the
   // first wave are claimed from it; the last CTA out zeroes it again.
   // Null: a fixed grid stride.
@@ -221,11 +226,17 @@ struct UmmaPlan {
   uint32_t NT, rps, imgp, plane_bytes, nbuf, z_off, img_off, rs_off, smem;
 };
 
-uint32_t umma_group_key(const MatchArgs& a);
+uint32_t umma_group_key(const MatchArgs& a);  // natural row width * 2 + masked
+// Natural tensor-memory row width (8..64) of templates w pixels wide.
+uint32_t umma_row_width(uint32_t w);
 // Sets every tensor-core kernel's shared-memory limit (outside stream capture).
 cudaError_t umma_prepare_kernels();
-// Plan of a batch group (launches of many tiles: the tallest tiles that fit).
-bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl);
+// Plan of a batch group (launches of many tiles): row width ks (8..64, a
+// power of two; 32 at most with a mask) and the tile height nt, or the
+// tallest tiles that fit when nt is 0. False when no plan fits.
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt = 0);
+// The tile heights a batch group can use, tallest first; returns the count.
+uint32_t umma_tile_heights(bool masked, uint32_t out[2]);
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
                          unsigned long long* ext_keys);
 uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl);
@@ -233,7 +244,8 @@ uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl);
 // err, tag set by the caller).
 cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t stream, KernelTimer* timer);
 cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s);
-cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const uint32_t* widths,
+// The finish kernel writes the records and re-arms the keys for the next launch.
+cudaError_t launch_extremes_keys_finish(unsigned long long* keys, const uint32_t* widths,
                                         ipb_extremes_f32* const* outs, uint32_t n, cudaStream_t s);
 
 // ---- many templates of one size against one image (tm_many.cu) ------------

@@ -445,12 +445,23 @@ __global__ void __launch_bounds__(256) head_train_kernel(const uint4* __restrict
   }
 }
 
-// per template (one block): loss_t = logsumexp(z_t) - z_t[pos_t];
-// z_t <- dz_t = (softmax(z_t) - onehot(pos_t)) / T
-__global__ void __launch_bounds__(1024) softmax_ce_kernel(float* __restrict__ z, size_t P,
+// per template (one block): with N_t the 3 x 3 neighbourhood of the positive
+// pos_t inside its crop (a position one step from the target is as good a
+// proposal, and the smooth scenes make neighbours nearly equal),
+//   loss_t = logsumexp_{all p}(z_t) - logsumexp_{p in N_t}(z_t),
+//   z_t <- dz_t = (softmax_all(z_t) - [p in N_t] softmax_{N_t}(z_t)) / T.
+__device__ __forceinline__ bool in_nbhd(size_t p, size_t pt, uint32_t H, uint32_t W) {
+  const size_t hw = (size_t)H * W;
+  if (p / hw != pt / hw) return false;
+  const int y = (int)((p % hw) / W), x = (int)(p % W), py = (int)((pt % hw) / W), px = (int)(pt % W);
+  return y - py <= 1 && py - y <= 1 && x - px <= 1 && px - x <= 1;
+}
+
+__global__ void __launch_bounds__(1024) softmax_ce_kernel(float* __restrict__ z, size_t P, uint32_t H, uint32_t W,
                                                           const int64_t* __restrict__ pos, uint32_t T,
                                                           float* __restrict__ loss) {
   __shared__ float s_red[32];
+  __shared__ float s_lsen;
   float* zt = z + (size_t)blockIdx.x * P;
   float mx = -INFINITY;
   for (size_t i = threadIdx.x; i < P; i += blockDim.x) mx = fmaxf(mx, zt[i]);
@@ -479,11 +490,35 @@ __global__ void __launch_bounds__(1024) softmax_ce_kernel(float* __restrict__ z,
   const float lse = mx + logf(s_red[0]);
   const int64_t pt = pos[blockIdx.x];
   const bool pos_ok = pt >= 0 && (size_t)pt < P;  // an out-of-range positive makes the loss NaN
-  const float zpos = pos_ok ? zt[pt] : NAN;
+  if (threadIdx.x == 0) {
+    float lsen = NAN;
+    if (pos_ok) {
+      const size_t hw = (size_t)H * W, base = (size_t)pt - (size_t)pt % hw;
+      const int py = (int)(((size_t)pt % hw) / W), px = (int)((size_t)pt % W);
+      float m = -INFINITY;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          if (py + dy >= 0 && py + dy < (int)H && px + dx >= 0 && px + dx < (int)W)
+            m = fmaxf(m, zt[base + (size_t)(py + dy) * W + px + dx]);
+      float e = 0.f;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          if (py + dy >= 0 && py + dy < (int)H && px + dx >= 0 && px + dx < (int)W)
+            e += expf(zt[base + (size_t)(py + dy) * W + px + dx] - m);
+      lsen = m + logf(e);
+    }
+    s_lsen = lsen;
+  }
   __syncthreads();
+  const float lsen = s_lsen;
   const float inv = 1.0f / (float)T;
-  for (size_t i = threadIdx.x; i < P; i += blockDim.x) zt[i] = expf(zt[i] - lse) * inv - (i == (size_t)pt ? inv : 0.f);
-  if (threadIdx.x == 0) atomicAdd(loss, (lse - zpos) * inv);
+  for (size_t i = threadIdx.x; i < P; i += blockDim.x) {
+    const float zi = zt[i];
+    float d = expf(zi - lse);
+    if (pos_ok && in_nbhd(i, (size_t)pt, H, W)) d -= expf(zi - lsen);
+    zt[i] = d * inv;
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, (lse - lsen) * inv);
 }
 
 // dF[q][c] = alpha sum_o sum_t dz[t][q - o] G[t][o][c] (bf16, row-chunked)
@@ -628,14 +663,17 @@ cudaError_t launch_conv_mma(const uint4* in, uint32_t n, uint32_t H, uint32_t W,
 }
 
 cudaError_t launch_trunk(const uint8_t* img, uint32_t n, uint32_t h, uint32_t w, const PackedWeights& pw,
-                         uint4* const* acts, uint4* tmp_a, uint4* tmp_b, uint4* F, cudaStream_t s) {
+                         uint4* const* acts, uint4* tmp_a, uint4* tmp_b, uint4* F, cudaStream_t s, int kernel,
+                         unsigned int* err, unsigned int tag) {
   const uint32_t H = h / 4, W = w / 4;
   uint4* cur = acts ? acts[0] : tmp_a;
   cudaError_t e = launch_conv1(img, n, h, w, pw.w1, pw.bias, cur, s);
   for (int l = 1; l < kLayers && e == cudaSuccess; ++l) {
     uint4* nxt = l == kLayers - 1 ? F : (acts ? acts[l] : (cur == tmp_a ? tmp_b : tmp_a));
-    e = launch_conv_mma(cur, n, H, W, pw.fwd + (size_t)(l - 1) * 9 * kC * kC, pw.bias + l * kC,
-                        l < kLayers - 1 ? 1 : 0, nullptr, nxt, s);
+    const uint16_t* wt = pw.fwd + (size_t)(l - 1) * 9 * kC * kC;
+    const int relu = l < kLayers - 1 ? 1 : 0;
+    e = kernel == 0 ? launch_conv_tc(cur, n, H, W, wt, pw.bias + l * kC, relu, nxt, err, tag, s)
+                    : launch_conv_mma(cur, n, H, W, wt, pw.bias + l * kC, relu, nullptr, nxt, s);
     cur = nxt;
   }
   return e;
@@ -803,7 +841,7 @@ ipb_status loss_and_grads(ipb_proposal_net* net, const uint8_t* scenes, uint32_t
   head_train_kernel<<<nblk, 256, head_smem, s>>>(c.Fs, N, H, W, c.G, T, c.z);
   count_launch(kKernelLearned);
   NET_CUDA(cudaGetLastError(), "head");
-  softmax_ce_kernel<<<T, 1024, 0, s>>>(c.z, P, pos, T, c.loss);
+  softmax_ce_kernel<<<T, 1024, 0, s>>>(c.z, P, H, W, pos, T, c.loss);
   count_launch(kKernelLearned);
   NET_CUDA(cudaGetLastError(), "loss");
   const size_t gf_smem = sizeof(float) * (T * kEmb + 4 * kHeadPos * T);
@@ -927,5 +965,28 @@ IPB_API ipb_status ipb_proposal_net_train_step(ipb_proposal_net* net, const uint
   count_launch(kKernelLearned);
   NET_CUDA(cudaGetLastError(), "adam");
   NET_CUDA(launch_pack_weights(net->params, net->pw, s), "pack weights");
+  return IPB_OK;
+}
+
+IPB_API ipb_status ipb_proposal_net_features(ipb_proposal_net* net, const uint8_t* d_image, uint32_t width,
+                                             uint32_t height, int kernel, void* d_out, void* stream) {
+  if (!net || !d_image || !d_out) return net_fail(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (width % 4 || height % 4 || width == 0 || height == 0)
+    return net_fail(IPB_ERR_INVALID_ARGUMENT, "image sides must be non-zero multiples of 4");
+  if (kernel != 0 && kernel != 1) return net_fail(IPB_ERR_INVALID_ARGUMENT, "kernel must be 0 or 1");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = 2 * align_up(act_units(1, height / 4, width / 4) * 16, 256);
+  if (net->scratch_bytes < bytes) {
+    NET_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (net->scratch) cudaFree(net->scratch);
+    net->scratch = nullptr;
+    net->scratch_bytes = 0;
+    NET_CUDA(cudaMalloc(&net->scratch, bytes), "cudaMalloc (feature scratch)");
+    net->scratch_bytes = bytes;
+  }
+  uint4* a = static_cast<uint4*>(net->scratch);
+  uint4* b = a + bytes / 2 / 16;
+  NET_CUDA(launch_trunk(d_image, 1, height, width, net->pw, nullptr, a, b, static_cast<uint4*>(d_out), s, kernel),
+           "trunk");
   return IPB_OK;
 }

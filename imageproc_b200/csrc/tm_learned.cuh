@@ -61,10 +61,22 @@ cudaError_t launch_conv1(const uint8_t* img, uint32_t n, uint32_t h, uint32_t w,
 // accumulation: out = bf16(act(bias + conv(wt, in))) [* (mask > 0)]
 cudaError_t launch_conv_mma(const uint4* in, uint32_t n, uint32_t H, uint32_t W, const uint16_t* wt,
                             const float* bias, int relu, const uint4* mask, uint4* out, cudaStream_t s);
+// the same convolution on tcgen05 (kind::f16, accumulators in tensor memory):
+// out = bf16(act(bias + conv(wt, in))); a bounded wait that runs out stores
+// `tag` into *err (when err is not null)
+cudaError_t launch_conv_tc(const uint4* in, uint32_t n, uint32_t H, uint32_t W, const uint16_t* wt,
+                           const float* bias, int relu, uint4* out, unsigned int* err, unsigned int tag,
+                           cudaStream_t s);
 // the trunk: conv1 + four tensor-core layers; acts (4 buffers) keeps A1..A4
-// when not null (training), otherwise ping-pong buffers a/b are used
+// when not null (training), otherwise ping-pong buffers a/b are used.
+// kernel: 0 = tcgen05 (launch_conv_tc), 1 = mma.sync (launch_conv_mma)
 cudaError_t launch_trunk(const uint8_t* img, uint32_t n, uint32_t h, uint32_t w, const PackedWeights& pw,
-                         uint4* const* acts, uint4* tmp_a, uint4* tmp_b, uint4* F, cudaStream_t s);
+                         uint4* const* acts, uint4* tmp_a, uint4* tmp_b, uint4* F, cudaStream_t s,
+                         int kernel = 1, unsigned int* err = nullptr, unsigned int tag = 0);
+// heatmap cell maxima on tcgen05: cells[t][cy][cx] = max over the cell's 8 x 8
+// positions of (order key of z_t << 32) | ~position (gb: [4][T][32] bf16)
+cudaError_t launch_head_tc(const uint4* F, uint32_t Hs, uint32_t Ws, const uint16_t* gb, uint32_t T,
+                           unsigned long long* cells, unsigned int* err, unsigned int tag, cudaStream_t s);
 // G[t][o * 32 + c] (fp32) from the templates' 12 x 12 feature maps
 cudaError_t launch_embed(const uint4* Ft, uint32_t T, float* G, cudaStream_t s);
 

@@ -29,6 +29,7 @@
 // exactly: every position outside the verified set has a larger score.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -44,10 +45,10 @@ namespace learned {
 namespace {
 
 constexpr int kCell = 8;          // heatmap cell: 8 x 8 downsampled positions
-constexpr int kMaxTopK = 32;
+constexpr int kMaxTopK = 16;
 constexpr int kWin = 32;          // verification window: 32 x 32 positions
 constexpr int kBlk = 12;          // certification block: 12 x 12 positions
-constexpr int kMaxExtra = 256;    // most extra blocks a template may verify
+constexpr int kMaxExtra = 512;    // most extra 4 x 4 blocks a template may verify
 constexpr int kPatch = kWin + kTpl - 1;        // 79 image rows / columns per window
 constexpr int kPatchPitch = 96;                // 16-byte multiple >= kPatch + 4
 
@@ -235,38 +236,61 @@ __device__ __forceinline__ float block_sum(float v, float* red) {
   return red[32];
 }
 
-// One block (1024 threads) per template: repeated block maxima over the cells
-// (a selected cell is excluded by its index), then the softmax over all cells.
-__global__ void __launch_bounds__(1024) topk_kernel(const unsigned long long* __restrict__ cells, uint32_t Cy,
+// One block (512 threads) per template. One pass over the cells: every
+// thread keeps the 16 largest keys it sees, sorted, in registers; then k
+// block-wide maxima over the threads' list heads merge them (the owner of
+// each maximum shifts its list). Keys are distinct (they hold the position).
+// A second pass gives the softmax over all cells.
+__global__ void __launch_bounds__(512) topk_kernel(const unsigned long long* __restrict__ cells, uint32_t Cy,
                                                     uint32_t Cx, uint32_t W, uint32_t k, TopK* __restrict__ out) {
   __shared__ unsigned long long red[33];
   __shared__ float redf[33];
   __shared__ uint32_t sel_cell[kMaxTopK];
   const unsigned long long* ct = cells + (size_t)blockIdx.x * Cy * Cx;
   const uint32_t nc = Cy * Cx;
+  unsigned long long top[kMaxTopK];
+  uint32_t topi[kMaxTopK];
+#pragma unroll
+  for (int j = 0; j < kMaxTopK; ++j) {
+    top[j] = 0ull;
+    topi[j] = 0u;
+  }
+  for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
+    unsigned long long v = ct[i];
+    uint32_t vi = i;
+    if (v <= top[kMaxTopK - 1]) continue;
+    // insert: carry the new key down the sorted list
+#pragma unroll
+    for (int j = 0; j < kMaxTopK; ++j) {
+      if (v > top[j]) {
+        const unsigned long long t = top[j];
+        const uint32_t ti = topi[j];
+        top[j] = v;
+        topi[j] = vi;
+        v = t;
+        vi = ti;
+      }
+    }
+  }
   TopK r;
   r.count = 0;
   for (uint32_t round = 0; round < k; ++round) {
-    unsigned long long best = 0ull;
-    uint32_t best_i = 0xFFFFFFFFu;
-    for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
-      bool taken = false;
-      for (uint32_t q = 0; q < round; ++q) taken |= sel_cell[q] == i;
-      const unsigned long long v = taken ? 0ull : ct[i];
-      if (v > best) {
-        best = v;
-        best_i = i;
-      }
-    }
-    const unsigned long long m = block_max_u64(best, red);
+    const unsigned long long m = block_max_u64(top[0], red);
     if (m == 0ull) break;
-    // the owner of the maximum records its cell (keys are distinct: they hold the position)
-    if (best == m) sel_cell[round] = best_i;
-    __syncthreads();
+    if (top[0] == m) {
+      sel_cell[round] = topi[0];
+#pragma unroll
+      for (int j = 0; j + 1 < kMaxTopK; ++j) {
+        top[j] = top[j + 1];
+        topi[j] = topi[j + 1];
+      }
+      top[kMaxTopK - 1] = 0ull;
+    }
     r.pos[round] = 0xFFFFFFFFu - (uint32_t)(m & 0xFFFFFFFFu);
     r.logit[round] = okey_value((uint32_t)(m >> 32));
     r.count = round + 1;
   }
+  __syncthreads();
   // margin: softmax probability of the best cell minus that of the best cell
   // that is not one of its 8 neighbours
   float margin = 0.f;
@@ -313,7 +337,7 @@ __global__ void __launch_bounds__(256) verify_kernel(const uint8_t* __restrict__
   __shared__ unsigned long long s_best[8];
   __shared__ unsigned long long s_tss;
   const uint32_t t = blockIdx.y;
-  if (blockIdx.x >= counts[t]) return;
+  if (blockIdx.x >= min(counts[t], max_rects)) return;
   const Rect rc = rects[(size_t)t * max_rects + blockIdx.x];
   const uint32_t Wo = W - kTpl + 1;
   const uint8_t* tp = tpl + (size_t)t * kTpl * kTpl;
@@ -406,7 +430,7 @@ __global__ void __launch_bounds__(256) verify_kernel(const uint8_t* __restrict__
 // proposal's full-resolution estimate 4 (p - 5) + 2, moved inside the map
 __global__ void windows_kernel(const TopK* __restrict__ tk, uint32_t T, uint32_t Ws, uint32_t Wo, uint32_t Ho,
                                Rect* __restrict__ rects, uint32_t* __restrict__ counts, uint32_t max_rects,
-                               unsigned long long* __restrict__ best) {
+                               unsigned long long* __restrict__ best, uint32_t* __restrict__ n_extra) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T) return;
   const TopK& r = tk[t];
@@ -420,96 +444,106 @@ __global__ void windows_kernel(const TopK* __restrict__ tk, uint32_t T, uint32_t
   }
   counts[t] = r.count;
   best[t] = ~0ull;
+  n_extra[t] = 0;
 }
 
 // ---- 4. certification tables ----------------------------------------------------------
-// Fine table: for each block (bx, by) of 12 x 12 box-sum origins q (q from 0
-// to W - 12, H - 12), the minimum and maximum of the 12 x 12 box sum B(q).
-// One block of threads per 4 x 4 fine blocks (48 x 48 origins).
-__global__ void __launch_bounds__(256) fine_table_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
-                                                         uint32_t Fx, uint32_t Fy, uint2* __restrict__ fine) {
-  __shared__ uint8_t s_img[48 + kBlk - 1][48 + kBlk - 1 + 1];
-  __shared__ uint32_t s_row[48 + kBlk - 1][48];
-  __shared__ uint32_t s_mn[16], s_mx[16];
-  const uint32_t qx0 = blockIdx.x * 48, qy0 = blockIdx.y * 48;
+// B(q) = the 12 x 12 box sum of the image at origin q (q.x <= W - 12, q.y <=
+// H - 12). The micro table holds, for every 4 x 4 block of origins (micro
+// block m = q / 4), the minimum and maximum of B over the block, packed as
+// min | max << 16 (B <= 36720 fits 16 bits). For a block of positions P
+// (4 x 4 positions at 4 P) and the template's 12 x 12 block b = (i, j), the
+// origins p + 12 b lie in micro block P + 3 b -- aligned, since 12 = 3 x 4.
+// Two coarser tables give the minimum and maximum over 4 x 4 micro blocks
+// (16 x 16 positions) and over 16 x 16 micro blocks (64 x 64 positions)
+// starting at each micro block.
+constexpr int kTile = 64;  // origins per table tile side (16 x 16 micro blocks)
+
+__global__ void __launch_bounds__(256) micro_table_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
+                                                          uint32_t Mx, uint32_t My, uint32_t* __restrict__ micro) {
+  __shared__ uint8_t s_img[kTile + kBlk - 1][kTile + kBlk - 1 + 1];
+  __shared__ uint16_t s_row[kTile + kBlk - 1][kTile];
+  const uint32_t qx0 = blockIdx.x * kTile, qy0 = blockIdx.y * kTile;
   const uint32_t Qx = W - kBlk + 1, Qy = H - kBlk + 1;  // box-sum origins
-  for (uint32_t i = threadIdx.x; i < 59 * 59; i += blockDim.x) {
-    const uint32_t r = i / 59, c = i % 59, y = qy0 + r, x = qx0 + c;
+  constexpr uint32_t kIn = kTile + kBlk - 1;            // 75
+  for (uint32_t i = threadIdx.x; i < kIn * kIn; i += blockDim.x) {
+    const uint32_t r = i / kIn, c = i % kIn, y = qy0 + r, x = qx0 + c;
     s_img[r][c] = (y < H && x < W) ? img[(size_t)y * W + x] : 0;
   }
-  if (threadIdx.x < 16) {
-    s_mn[threadIdx.x] = 0xFFFFFFFFu;
-    s_mx[threadIdx.x] = 0u;
-  }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < 59 * 48; i += blockDim.x) {
-    const uint32_t r = i / 48, c = i % 48;
-    uint32_t s = 0;
+  for (uint32_t i = threadIdx.x; i < kIn * kTile; i += blockDim.x) {
+    const uint32_t r = i / kTile, c = i % kTile;
+    uint32_t v = 0;
 #pragma unroll
-    for (int d = 0; d < kBlk; ++d) s += s_img[r][c + d];
-    s_row[r][c] = s;
+    for (int d = 0; d < kBlk; ++d) v += s_img[r][c + d];
+    s_row[r][c] = (uint16_t)v;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < 48 * 48; i += blockDim.x) {
-    const uint32_t r = i / 48, c = i % 48;
-    if (qy0 + r >= Qy || qx0 + c >= Qx) continue;
-    uint32_t s = 0;
+  // thread = micro block (16 x 16 per tile): 4 columns of 4 box sums each
+  const uint32_t mxl = threadIdx.x & 15, myl = threadIdx.x >> 4;
+  const uint32_t mx = blockIdx.x * 16 + mxl, my = blockIdx.y * 16 + myl;
+  if (mx >= Mx || my >= My) return;
+  uint32_t mn = 0xFFFFu, mxv = 0u;
+  for (uint32_t c = 4 * mxl; c < 4 * mxl + 4; ++c) {
+    if (qx0 + c >= Qx) break;
+    const uint32_t r0 = 4 * myl;
+    uint32_t v = 0;
 #pragma unroll
-    for (int d = 0; d < kBlk; ++d) s += s_row[r + d][c];
-    const uint32_t b = (r / kBlk) * 4 + c / kBlk;
-    atomicMin(&s_mn[b], s);
-    atomicMax(&s_mx[b], s);
-  }
-  __syncthreads();
-  if (threadIdx.x < 16) {
-    const uint32_t bx = blockIdx.x * 4 + (threadIdx.x & 3), by = blockIdx.y * 4 + (threadIdx.x >> 2);
-    if (bx < Fx && by < Fy) fine[(size_t)by * Fx + bx] = make_uint2(s_mn[threadIdx.x], s_mx[threadIdx.x]);
-  }
-}
-
-// Coarse table: min / max of the fine table over the 4 x 4 fine blocks
-// starting at each fine block (clipped at the edges).
-__global__ void coarse_table_kernel(const uint2* __restrict__ fine, uint32_t Fx, uint32_t Fy,
-                                    uint2* __restrict__ coarse) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= Fx * Fy) return;
-  const uint32_t bx = i % Fx, by = i / Fx;
-  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
-  for (uint32_t dy = 0; dy < 4 && by + dy < Fy; ++dy)
-    for (uint32_t dx = 0; dx < 4 && bx + dx < Fx; ++dx) {
-      const uint2 v = fine[(size_t)(by + dy) * Fx + bx + dx];
-      mn = v.x < mn ? v.x : mn;
-      mx = v.y > mx ? v.y : mx;
+    for (int d = 0; d < kBlk; ++d) v += s_row[r0 + d][c];
+    for (uint32_t r = r0; r < r0 + 4 && qy0 + r < Qy; ++r) {
+      if (r > r0) v += (uint32_t)s_row[r + kBlk - 1][c] - (uint32_t)s_row[r - 1][c];
+      mn = v < mn ? v : mn;
+      mxv = v > mxv ? v : mxv;
     }
-  coarse[i] = make_uint2(mn, mx);
+  }
+  micro[(size_t)my * Mx + mx] = mn | (mxv << 16);
 }
 
-// ---- 4b. certification of one template (one block per template) ---------------------------
-// status: 0 certified (extra rectangles, if any, still to verify), 1 low
-// margin, 2 too many uncertified blocks
-__device__ __forceinline__ unsigned long long lb_term(uint32_t st, uint2 mm) {
-  const uint32_t d = st < mm.x ? mm.x - st : (st > mm.y ? st - mm.y : 0u);
+// out[m] = min / max of in over the 4 x 4 entries in[m + step * (a, b)],
+// a, b = 0..3 (clipped at the edges)
+__global__ void span_table_kernel(const uint32_t* __restrict__ in, uint32_t Mx, uint32_t My, uint32_t step,
+                                  uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Mx * My) return;
+  const uint32_t x = i % Mx, y = i / Mx;
+  uint32_t mn = 0xFFFFu, mx = 0u;
+  for (uint32_t b = 0; b < 4 && y + step * b < My; ++b)
+    for (uint32_t a = 0; a < 4 && x + step * a < Mx; ++a) {
+      const uint32_t v = in[(size_t)(y + step * b) * Mx + x + step * a];
+      mn = min(mn, v & 0xFFFFu);
+      mx = max(mx, v >> 16);
+    }
+  out[i] = mn | (mx << 16);
+}
+
+// ---- 4b. certification of one template -------------------------------------------------
+__device__ __forceinline__ unsigned long long lb_term(uint32_t st, uint32_t packed) {
+  const uint32_t lo = packed & 0xFFFFu, hi = packed >> 16;
+  const uint32_t d = st < lo ? lo - st : (st > hi ? st - hi : 0u);
   return (unsigned long long)d * d;
 }
 
-__global__ void __launch_bounds__(1024) certify_kernel(const uint8_t* __restrict__ tpl, const TopK* __restrict__ tk,
-                                                       float min_margin, const unsigned long long* __restrict__ best,
-                                                       const uint2* __restrict__ fine, const uint2* __restrict__ coarse,
-                                                       uint32_t Fx, uint32_t Fy, uint32_t Wo, uint32_t Ho,
-                                                       const Rect* __restrict__ wins, const uint32_t* __restrict__ nwin,
-                                                       uint32_t max_rects, Rect* __restrict__ extra,
-                                                       uint32_t* __restrict__ n_extra, uint32_t* __restrict__ status) {
+constexpr int kCertSlices = 16;  // blocks of threads per template
+
+// Grid (template, slice): each block takes every kCertSlices-th block of
+// 64 x 64 positions. A block whose lower bound exceeds the verified minimum is
+// excluded; the others split into 16 blocks of 16 x 16, and those into 16
+// micro blocks of 4 x 4 positions. A micro block that is neither excluded nor
+// inside a verified window is appended to the template's extra list (counter
+// n_extra[t], zeroed by windows_kernel); a count above kMaxExtra means the
+// template falls back.
+__global__ void __launch_bounds__(256) certify_kernel(const uint8_t* __restrict__ tpl, const TopK* __restrict__ tk,
+                                                      float min_margin, const unsigned long long* __restrict__ best,
+                                                      const uint32_t* __restrict__ micro,
+                                                      const uint32_t* __restrict__ span4,
+                                                      const uint32_t* __restrict__ span16, uint32_t Mx, uint32_t My,
+                                                      uint32_t Wo, uint32_t Ho, const Rect* __restrict__ wins,
+                                                      const uint32_t* __restrict__ nwin, uint32_t max_rects,
+                                                      Rect* __restrict__ extra, uint32_t* __restrict__ n_extra) {
   __shared__ uint32_t s_st[16];
   __shared__ Rect s_win[kMaxTopK];
-  __shared__ uint32_t s_count;
   const uint32_t t = blockIdx.x;
-  if (tk[t].margin < min_margin || tk[t].count == 0) {
-    if (threadIdx.x == 0) {
-      status[t] = 1;
-      n_extra[t] = 0;
-    }
-    return;
-  }
+  if (tk[t].margin < min_margin || tk[t].count == 0) return;
   const uint8_t* tp = tpl + (size_t)t * kTpl * kTpl;
   if (threadIdx.x < 16) {
     const uint32_t by = threadIdx.x >> 2, bx = threadIdx.x & 3;
@@ -520,52 +554,47 @@ __global__ void __launch_bounds__(1024) certify_kernel(const uint8_t* __restrict
   }
   const uint32_t nw = nwin[t];
   if (threadIdx.x < nw) s_win[threadIdx.x] = wins[(size_t)t * max_rects + threadIdx.x];
-  if (threadIdx.x == 0) s_count = 0;
   __syncthreads();
   // the verified minimum; a block is excluded when RN_f32(ceil(LB)) > it
   const float sstar = okey_value((uint32_t)(best[t] >> 32));
-  const uint32_t Px = (Wo + kBlk - 1) / kBlk, Py = (Ho + kBlk - 1) / kBlk;  // position blocks
-  const uint32_t Cqx = (Px + 3) / 4, Cqy = (Py + 3) / 4;
   auto excluded = [&](unsigned long long num) {
     const unsigned long long lb = (num + 143ull) / 144ull;  // SSE is an integer >= num / 144
     return (float)lb > sstar;
   };
-  for (uint32_t q = threadIdx.x; q < Cqx * Cqy; q += blockDim.x) {
-    const uint32_t qx = q % Cqx, qy = q / Cqx;
+  // lower bound of a block of positions starting at micro block (px, py),
+  // template block b at micro offset 3 * b, from `table`
+  auto bound = [&](const uint32_t* table, uint32_t px, uint32_t py) {
     unsigned long long num = 0ull;
 #pragma unroll
     for (int b = 0; b < 16; ++b) {
-      const uint32_t fx = 4 * qx + (b & 3), fy = 4 * qy + (b >> 2);
-      if (fx < Fx && fy < Fy) num += lb_term(s_st[b], coarse[(size_t)fy * Fx + fx]);
+      const uint32_t mx = px + 3 * (b & 3), my = py + 3 * (b >> 2);
+      if (mx < Mx && my < My) num += lb_term(s_st[b], table[(size_t)my * Mx + mx]);
     }
-    if (excluded(num)) continue;
-    for (uint32_t k = 0; k < 16; ++k) {
-      const uint32_t bx = 4 * qx + (k & 3), by = 4 * qy + (k >> 2);
-      if (bx >= Px || by >= Py) continue;
-      unsigned long long n2 = 0ull;
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const uint32_t fx = bx + (b & 3), fy = by + (b >> 2);
-        if (fx < Fx && fy < Fy) n2 += lb_term(s_st[b], fine[(size_t)fy * Fx + fx]);
+    return num;
+  };
+  const uint32_t Pmx = (Wo + 3) / 4, Pmy = (Ho + 3) / 4;  // micro blocks of positions
+  const uint32_t C3x = (Pmx + 15) / 16, C3y = (Pmy + 15) / 16;
+  for (uint32_t q = blockIdx.y * blockDim.x + threadIdx.x; q < C3x * C3y; q += gridDim.y * blockDim.x) {
+    const uint32_t p3x = 16 * (q % C3x), p3y = 16 * (q / C3x);
+    if (excluded(bound(span16, p3x, p3y))) continue;
+    for (uint32_t k2 = 0; k2 < 16; ++k2) {
+      const uint32_t p2x = p3x + 4 * (k2 & 3), p2y = p3y + 4 * (k2 >> 2);
+      if (p2x >= Pmx || p2y >= Pmy || excluded(bound(span4, p2x, p2y))) continue;
+      for (uint32_t k1 = 0; k1 < 16; ++k1) {
+        const uint32_t px = p2x + (k1 & 3), py = p2y + (k1 >> 2);
+        if (px >= Pmx || py >= Pmy || excluded(bound(micro, px, py))) continue;
+        const uint32_t x0 = 4 * px, y0 = 4 * py;
+        const uint32_t x1 = min(x0 + 4, Wo), y1 = min(y0 + 4, Ho);
+        bool covered = false;
+        for (uint32_t w = 0; w < nw && !covered; ++w) {
+          const Rect r = s_win[w];
+          covered = x0 >= r.x0 && y0 >= r.y0 && x1 <= r.x0 + r.w && y1 <= r.y0 + r.h;
+        }
+        if (covered) continue;
+        const uint32_t slot = atomicAdd(n_extra + t, 1u);
+        if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = Rect{x0, y0, x1 - x0, y1 - y0};
       }
-      if (excluded(n2)) continue;
-      const uint32_t x0 = bx * kBlk, y0 = by * kBlk;
-      const uint32_t x1 = min(x0 + kBlk, Wo), y1 = min(y0 + kBlk, Ho);
-      bool covered = false;
-      for (uint32_t w = 0; w < nw && !covered; ++w) {
-        const Rect r = s_win[w];
-        covered = x0 >= r.x0 && y0 >= r.y0 && x1 <= r.x0 + r.w && y1 <= r.y0 + r.h;
-      }
-      if (covered) continue;
-      const uint32_t slot = atomicAdd(&s_count, 1u);
-      if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = Rect{x0, y0, x1 - x0, y1 - y0};
     }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const uint32_t c = s_count;
-    status[t] = c > kMaxExtra ? 2u : 0u;
-    n_extra[t] = c > kMaxExtra ? 0u : c;
   }
 }
 
@@ -636,10 +665,10 @@ struct Carve {
   uint32_t* nwin;
   Rect* extra;
   uint32_t* n_extra;
-  uint32_t* status;
   unsigned long long* best;
-  uint2* fine;
-  uint2* coarse;
+  uint32_t* micro;
+  uint32_t* span4;
+  uint32_t* span16;
   uint8_t* fb_tpl;
   unsigned long long* fb_keys;
   ipb_extremes_f32* fb_ext;
@@ -671,16 +700,27 @@ Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
   c.nwin = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
   c.extra = reinterpret_cast<Rect*>(take((size_t)T * kMaxExtra * sizeof(Rect)));
   c.n_extra = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
-  c.status = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
   c.best = reinterpret_cast<unsigned long long*>(take((size_t)T * 8));
-  const uint32_t Fx = (W - kBlk + 1 + kBlk - 1) / kBlk, Fy = (H - kBlk + 1 + kBlk - 1) / kBlk;
-  c.fine = reinterpret_cast<uint2*>(take((size_t)Fx * Fy * 8));
-  c.coarse = reinterpret_cast<uint2*>(take((size_t)Fx * Fy * 8));
+  const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
+  c.micro = reinterpret_cast<uint32_t*>(take((size_t)Mx * My * 4));
+  c.span4 = reinterpret_cast<uint32_t*>(take((size_t)Mx * My * 4));
+  c.span16 = reinterpret_cast<uint32_t*>(take((size_t)Mx * My * 4));
   c.fb_tpl = reinterpret_cast<uint8_t*>(take((size_t)T * kTpl * kTpl));
   c.fb_keys = reinterpret_cast<unsigned long long*>(take((size_t)T * 16));
   c.fb_ext = reinterpret_cast<ipb_extremes_f32*>(take((size_t)T * sizeof(ipb_extremes_f32)));
   c.bytes = off;
   return c;
+}
+
+// IPB_LEARNED_KERNELS=mma runs the query's convolutions and heatmap on the
+// mma.sync kernels of the training path instead of tcgen05 (same arithmetic:
+// bf16 operands, fp32 accumulation); for testing and measurement.
+bool use_mma_kernels() {
+  static const bool v = [] {
+    const char* e = std::getenv("IPB_LEARNED_KERNELS");
+    return e && std::strcmp(e, "mma") == 0;
+  }();
+  return v;
 }
 
 ProposeScratch& scratch_for_thread() {
@@ -709,7 +749,7 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
   ipb_propose_options opt{16u, 0.1f, 1};
   if (options) opt = *options;
   if (opt.top_k == 0 || opt.top_k > (uint32_t)kMaxTopK)
-    return pfail(IPB_ERR_INVALID_ARGUMENT, "top_k must be 1..32");
+    return pfail(IPB_ERR_INVALID_ARGUMENT, "top_k must be 1..16");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   ProposeScratch& ps = scratch_for_thread();
   int dev = 0;
@@ -738,35 +778,49 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
   const PackedWeights& pw = net_weights(net);
   const uint32_t Hs = H / 4, Ws = W / 4, Wo = W - kTpl + 1, Ho = H - kTpl + 1;
   const uint32_t Cx = Ws / kCell, Cy = Hs / kCell;
-  const uint32_t Fx = (W - kBlk + 1 + kBlk - 1) / kBlk, Fy = (H - kBlk + 1 + kBlk - 1) / kBlk;
+  const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
 
   // 1. trunk of the image and of the templates, embedding, heatmap cells
-  P_CUDA(launch_trunk(d_image, 1, H, W, pw, nullptr, c.a, c.b, c.F, s), "image trunk");
-  P_CUDA(launch_trunk(d_templates, T, kTpl, kTpl, pw, nullptr, c.ta, c.tb, c.Ft, s), "template trunk");
+  // one tag for every tensor-core launch of this call: a bounded wait that runs
+  // out in any of them leaves a value >= it in the error word
+  const unsigned int call_tag = ++ps.tag;
+  const int conv_kernel = use_mma_kernels() ? 1 : 0;
+  P_CUDA(launch_trunk(d_image, 1, H, W, pw, nullptr, c.a, c.b, c.F, s, conv_kernel, ps.err, call_tag),
+         "image trunk");
+  P_CUDA(launch_trunk(d_templates, T, kTpl, kTpl, pw, nullptr, c.ta, c.tb, c.Ft, s, conv_kernel, ps.err, call_tag),
+         "template trunk");
   P_CUDA(launch_embed(c.Ft, T, c.G, s), "embedding");
   pack_embedding_kernel<<<(T * kEmb + 255) / 256, 256, 0, s>>>(c.G, T, c.gb);
   count_launch(kKernelPropose);
-  const dim3 hg((Ws + kHW - 1) / kHW, Hs / kCell, (T + 31) / 32);
-  head_cells_kernel<<<hg, 256, 0, s>>>(c.F, Hs, Ws, c.gb, T, c.cells);
-  count_launch(kKernelPropose);
-  P_CUDA(cudaGetLastError(), "heatmap");
+  if (use_mma_kernels()) {
+    const dim3 hg((Ws + kHW - 1) / kHW, Hs / kCell, (T + 31) / 32);
+    head_cells_kernel<<<hg, 256, 0, s>>>(c.F, Hs, Ws, c.gb, T, c.cells);
+    count_launch(kKernelPropose);
+    P_CUDA(cudaGetLastError(), "heatmap");
+  } else {
+    P_CUDA(launch_head_tc(c.F, Hs, Ws, c.gb, T, c.cells, ps.err, call_tag, s), "heatmap");
+  }
   // 2. top-k and margins
-  topk_kernel<<<T, 1024, 0, s>>>(c.cells, Cy, Cx, Ws, opt.top_k, c.tk);
+  topk_kernel<<<T, 512, 0, s>>>(c.cells, Cy, Cx, Ws, opt.top_k, c.tk);
   count_launch(kKernelPropose);
   // 3. windows and their exact scores
-  windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(c.tk, T, Ws, Wo, Ho, c.wins, c.nwin, opt.top_k, c.best);
+  windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(c.tk, T, Ws, Wo, Ho, c.wins, c.nwin, opt.top_k, c.best,
+                                                 c.n_extra);
   count_launch(kKernelPropose);
   verify_kernel<<<dim3(opt.top_k, T), 256, 0, s>>>(d_image, W, H, d_templates, c.wins, c.nwin, opt.top_k, c.best);
   count_launch(kKernelPropose);
   P_CUDA(cudaGetLastError(), "verification");
   // 4. certification
   if (opt.certify) {
-    fine_table_kernel<<<dim3((Fx + 3) / 4, (Fy + 3) / 4), 256, 0, s>>>(d_image, W, H, Fx, Fy, c.fine);
+    micro_table_kernel<<<dim3((Mx + 15) / 16, (My + 15) / 16), 256, 0, s>>>(d_image, W, H, Mx, My, c.micro);
     count_launch(kKernelPropose);
-    coarse_table_kernel<<<(Fx * Fy + 255) / 256, 256, 0, s>>>(c.fine, Fx, Fy, c.coarse);
+    span_table_kernel<<<(Mx * My + 255) / 256, 256, 0, s>>>(c.micro, Mx, My, 1, c.span4);
     count_launch(kKernelPropose);
-    certify_kernel<<<T, 1024, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.fine, c.coarse, Fx, Fy, Wo, Ho,
-                                      c.wins, c.nwin, opt.top_k, c.extra, c.n_extra, c.status);
+    span_table_kernel<<<(Mx * My + 255) / 256, 256, 0, s>>>(c.span4, Mx, My, 4, c.span16);
+    count_launch(kKernelPropose);
+    certify_kernel<<<dim3(T, kCertSlices), 256, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.micro, c.span4,
+                                                        c.span16, Mx, My, Wo, Ho, c.wins, c.nwin, opt.top_k,
+                                                        c.extra, c.n_extra);
     count_launch(kKernelPropose);
     verify_kernel<<<dim3(kMaxExtra, T), 256, 0, s>>>(d_image, W, H, d_templates, c.extra, c.n_extra, kMaxExtra,
                                                      c.best);
@@ -775,17 +829,25 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
   }
   // 5. the verdicts to the host; fallback templates through the exhaustive kernel
   std::vector<TopK> tk(T);
-  std::vector<uint32_t> status(T, 0u);
+  std::vector<uint32_t> status(T, 0u), n_extra(T, 0u);
   std::vector<unsigned long long> best(T);
   P_CUDA(cudaMemcpyAsync(tk.data(), c.tk, sizeof(TopK) * T, cudaMemcpyDeviceToHost, s), "copy proposals");
   P_CUDA(cudaMemcpyAsync(best.data(), c.best, sizeof(unsigned long long) * T, cudaMemcpyDeviceToHost, s),
          "copy scores");
   if (opt.certify)
-    P_CUDA(cudaMemcpyAsync(status.data(), c.status, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s), "copy status");
+    P_CUDA(cudaMemcpyAsync(n_extra.data(), c.n_extra, sizeof(uint32_t) * T, cudaMemcpyDeviceToHost, s),
+           "copy extra counts");
+  unsigned int failed = 0;
+  P_CUDA(cudaMemcpyAsync(&failed, ps.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "copy error word");
   P_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  if (failed >= call_tag)
+    return pfail(IPB_ERR_TIMEOUT, "a proposal-network convolution timed out waiting on its pipeline");
   std::vector<uint32_t> fb;
   for (uint32_t t = 0; t < T; ++t) {
-    if (!opt.certify && (tk[t].margin < opt.min_margin || tk[t].count == 0)) status[t] = 1;
+    if (tk[t].margin < opt.min_margin || tk[t].count == 0)
+      status[t] = 1;  // low margin: no verification counts
+    else if (opt.certify && n_extra[t] > (uint32_t)kMaxExtra)
+      status[t] = 2;  // too many blocks the bound cannot exclude
     if (status[t]) fb.push_back(t);
   }
   std::vector<ipb_extremes_f32> fb_ext(fb.size());
@@ -796,17 +858,15 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
              "gather fallback templates");
     const uint32_t nf = (uint32_t)fb.size();
     P_CUDA(launch_many_keys_init(c.fb_keys, nf, s), "extremes init");
-    ps.tag += 1;
     P_CUDA(launch_many(d_image, W, H, c.fb_tpl, kTpl, kTpl, nf, IPB_SUM_OF_SQUARED_ERRORS,
-                       IPB_PRECISION_EXACT_FP64, nullptr, c.fb_keys, ps.err, ps.tag, s, nullptr),
+                       IPB_PRECISION_EXACT_FP64, nullptr, c.fb_keys, ps.err, call_tag, s, nullptr),
            "exhaustive fallback");
     P_CUDA(launch_many_keys_finish(c.fb_keys, Wo, c.fb_ext, nf, s), "extremes finish");
-    unsigned int failed = 0;
     P_CUDA(cudaMemcpyAsync(fb_ext.data(), c.fb_ext, sizeof(ipb_extremes_f32) * nf, cudaMemcpyDeviceToHost, s),
            "copy fallback results");
     P_CUDA(cudaMemcpyAsync(&failed, ps.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "copy error word");
     P_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    if (failed >= ps.tag)
+    if (failed >= call_tag)
       return pfail(IPB_ERR_TIMEOUT, "the exhaustive fallback kernel timed out waiting on its pipeline");
   }
   size_t f = 0;
@@ -814,6 +874,7 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
     ipb_proposal_result& r = results[t];
     r.margin = tk[t].margin;
     r.path = status[t];
+    r.uncertified = n_extra[t];
     if (status[t]) {
       const ipb_extremes_f32& e = fb_ext[f++];
       r.value = e.min_value;

@@ -40,7 +40,7 @@ class ProposeOptions(C.Structure):
 
 class ProposalResult(C.Structure):
     _fields_ = [("value", C.c_float), ("x", C.c_uint32), ("y", C.c_uint32), ("margin", C.c_float),
-                ("path", C.c_uint32)]
+                ("path", C.c_uint32), ("uncertified", C.c_uint32)]
 
 
 @dataclass(frozen=True)
@@ -49,6 +49,7 @@ class Answer:
     location: tuple       # (x, y) of its first occurrence
     margin: float         # heatmap confidence margin
     path: int             # 0 proposals, 1 fallback (low margin), 2 fallback (not certified)
+    uncertified: int = 0  # 4 x 4 position blocks the certificate could not exclude
 
 
 def _bind():
@@ -64,8 +65,10 @@ def _bind():
                                               C.POINTER(C.c_float), vp]
     L.ipb_propose_and_match_device.argtypes = [vp, vp, u32, u32, vp, u32, u32, u32, C.c_int,
                                                C.POINTER(ProposeOptions), C.POINTER(ProposalResult), vp]
+    L.ipb_proposal_net_features.argtypes = [vp, vp, u32, u32, C.c_int, vp, vp]
     for f in ("ipb_proposal_net_create", "ipb_proposal_net_destroy", "ipb_proposal_net_get_params",
-              "ipb_proposal_net_gradients", "ipb_proposal_net_train_step", "ipb_propose_and_match_device"):
+              "ipb_proposal_net_gradients", "ipb_proposal_net_train_step", "ipb_propose_and_match_device",
+              "ipb_proposal_net_features"):
         getattr(L, f).restype = C.c_int
     L._learned_bound = True
     return L
@@ -160,6 +163,17 @@ class ProposalNet:
             positives.data_ptr(), C.c_float(lr), C.byref(loss), _stream(stream)))
         return float(loss.value)
 
+    def features(self, image: torch.Tensor, kernel: int = 0, stream=None) -> torch.Tensor:
+        """The network's 32-channel features of one image (sides multiples of 4),
+        as a (32, H/4, W/4) float32 tensor. kernel 0: tcgen05 (the query path),
+        1: mma.sync (the training path)."""
+        _u8(image, "image")
+        H, W = image.shape
+        raw = torch.empty((H // 4, 4, W // 4, 8), dtype=torch.bfloat16, device=image.device)
+        check(_bind().ipb_proposal_net_features(self._h, image.data_ptr(), W, H, int(kernel), raw.data_ptr(),
+                                                _stream(stream)))
+        return raw.permute(1, 3, 0, 2).reshape(32, H // 4, W // 4).float()
+
     def propose_and_match(self, image: torch.Tensor, templates: torch.Tensor, *, top_k: int = 16,
                           min_margin: float = 0.1, certify: bool = True, stream=None) -> list[Answer]:
         """SumOfSquaredErrors minimum of every 48 x 48 template (a (t, 48, 48)
@@ -170,10 +184,13 @@ class ProposalNet:
         n = templates.shape[0]
         res = (ProposalResult * max(n, 1))()
         opt = ProposeOptions(top_k, min_margin, int(certify))
+        if templates.dim() != 3:
+            raise ValueError("templates must be a (t, h, w) tensor")
+        th, tw = templates.shape[1], templates.shape[2]
         check(_bind().ipb_propose_and_match_device(
-            self._h, image.data_ptr(), W, H, templates.data_ptr(), TPL, TPL, n, 0, C.byref(opt), res,
+            self._h, image.data_ptr(), W, H, templates.data_ptr(), tw, th, n, 0, C.byref(opt), res,
             _stream(stream)))
-        return [Answer(float(r.value), (int(r.x), int(r.y)), float(r.margin), int(r.path))
+        return [Answer(float(r.value), (int(r.x), int(r.y)), float(r.margin), int(r.path), int(r.uncertified))
                 for r in res[:n]]
 
 
@@ -226,19 +243,24 @@ def training_batch(scenes: torch.Tensor, n: int, g: np.random.Generator, crop: i
 
 
 def train(net: ProposalNet, scenes: torch.Tensor, *, pairs: int = 200_000, batch: int = 128,
-          lr: float = 1e-3, seed: int = 0, log_every: int = 100, crop: int = 96, log=print) -> list[float]:
-    """Adam over `pairs` seeded (crop, template) pairs in batches of `batch`;
-    returns the per-step losses."""
-    g = np.random.default_rng(seed)
+          lr: float = 1e-3, seed: int = 0, log_every: int = 100, crop: int = 96, epochs: int = 1,
+          log=print) -> list[float]:
+    """Adam over `pairs` seeded (crop, template) pairs in batches of `batch`,
+    `epochs` passes over the same pairs (the generator restarts from `seed`
+    each pass); returns the per-step losses."""
     steps = (pairs + batch - 1) // batch
+    total = steps * epochs
     losses = []
-    for s in range(steps):
-        crops, templates, pos = training_batch(scenes, batch, g, crop)
-        # cosine decay to a tenth
-        lr_s = lr * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * s / max(1, steps))))
-        losses.append(net.train_step(crops, templates, pos, lr_s))
-        if log and (s % log_every == 0 or s == steps - 1):
-            log(f"step {s}/{steps} loss {np.mean(losses[-log_every:]):.4f} lr {lr_s:.2e}")
+    for e in range(epochs):
+        g = np.random.default_rng(seed)
+        for s in range(steps):
+            crops, templates, pos = training_batch(scenes, batch, g, crop)
+            k = e * steps + s
+            # cosine decay to a tenth over all passes
+            lr_s = lr * (0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * k / max(1, total))))
+            losses.append(net.train_step(crops, templates, pos, lr_s))
+            if log and (k % log_every == 0 or k == total - 1):
+                log(f"step {k}/{total} loss {np.mean(losses[-log_every:]):.4f} lr {lr_s:.2e}")
     return losses
 
 
@@ -251,13 +273,16 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--scenes", type=int, default=4)
     ap.add_argument("--side", type=int, default=8192)
+    ap.add_argument("--crop", type=int, default=96)
+    ap.add_argument("--epochs", type=int, default=1)
     ap.add_argument("--out", default=str(WEIGHTS))
     args = ap.parse_args(argv)
     torch.cuda.set_device(0)
     imgs = [training_scene(1000 + k, args.side) for k in range(args.scenes)]
     scenes = torch.from_numpy(np.stack(imgs)).cuda()
     net = ProposalNet(seed=args.seed)
-    losses = train(net, scenes, pairs=args.pairs, batch=args.batch, lr=args.lr, seed=args.seed)
+    losses = train(net, scenes, pairs=args.pairs, batch=args.batch, lr=args.lr, seed=args.seed,
+                   crop=args.crop, epochs=args.epochs)
     net.save(args.out)
     print(f"saved {args.out}; loss {np.mean(losses[:50]):.4f} -> {np.mean(losses[-50:]):.4f}")
 

@@ -117,11 +117,16 @@ def value_noise_scene(W=4096, H=4096, n_templates=512, t=32, seed=4, noise=6):
     return image, templates, locs
 
 
-def rect_scene(W=8192, H=8192, n_rects=500, n_templates=64, t=48, seed=5):
+def rect_scene(W=8192, H=8192, n_rects=500, n_templates=64, t=48, seed=5, max_side=256):
+    """Value noise plus n_rects flat rectangles (sides U{8..max_side - 1},
+    intensity U{0..255}) and n_templates t x t crops with a brightness offset
+    in [-10, 10] and noise in [-6, 6]. With the default sides, 500 rectangles
+    cover about 12 % of an 8192 x 8192 scene (sides up to 1024 would cover
+    about 82 % and cut most templates from flat regions)."""
     g = rng(seed + 2000)
     image = value_noise(W, H, seed)
     for _ in range(n_rects):
-        rw, rh = int(g.integers(8, W // 8)), int(g.integers(8, H // 8))
+        rw, rh = int(g.integers(8, max_side)), int(g.integers(8, max_side))
         x, y = int(g.integers(0, W - rw)), int(g.integers(0, H - rh))
         image[y:y + rh, x:x + rw] = np.uint8(g.integers(0, 256))
     templates = np.empty((n_templates, t, t), np.uint8)

@@ -141,6 +141,13 @@ int ipb_get_path(void);
  * Tests set a budget far below one tile's time to make a wait run out without
  * faulting or hanging the GPU. */
 void ipb_debug_set_pipeline_wait_ns(uint64_t ns);
+/* Failure-detection test hook (no counterpart in the reference): while
+ * enabled, the MMA-issuing warp of every tensor-core kernel launched
+ * afterwards first waits on a barrier that nothing arrives at, so its bounded
+ * wait runs out and the call reports IPB_ERR_TIMEOUT; pair it with a small
+ * budget from ipb_debug_set_pipeline_wait_ns to keep the test short. Nothing
+ * faults or spins without a limit. */
+void ipb_debug_stall_pipelines(int enable);
 
 /* ---- tracing -------------------------------------------------------------
  * No counterpart in the reference (which has no instrumentation); used by the
@@ -269,9 +276,17 @@ typedef struct ipb_pair {
 ipb_status ipb_match_template_batch_device(const ipb_pair *pairs, uint32_t n,
                                            int precision, void *stream);
 
-/* A reusable batch: pairs checked, kernel paths chosen (by the autotuner when
- * the environment variable IPB_AUTOTUNE=1, else by its cost model), device
+/* A reusable batch: pairs checked, kernel paths chosen, tensor-core pairs
+ * grouped into one launch per (row width, tile height, mask kind), device
  * descriptors uploaded and the launch sequence captured in a CUDA graph.
+ * Autotuning (environment variable IPB_AUTOTUNE): unset, each group's row
+ * width (its natural width or twice it) and tile height are timed on the
+ * group's own pairs the first time a group of that class is planned, so plan
+ * creation may run the pairs and write their outputs; IPB_AUTOTUNE=1 also
+ * times tensor cores against the CUDA-core kernel per template shape class;
+ * IPB_AUTOTUNE=0 uses the cost model alone. Decisions are cached per process
+ * and persisted in IPB_TUNING_FILE (default ~/.cache/imageproc_b200/
+ * tuning.txt; an empty value keeps them in memory).
  * Pointers in `pairs` must stay valid for the plan's life; launching replays
  * the graph on `stream`. Tensor-core groups run side by side inside the graph
  * (a fork to the plan's own stream and a join back), so the launch is ordered
@@ -285,6 +300,20 @@ ipb_status ipb_batch_plan_launch(ipb_batch_plan *plan, void *stream);
 /* Kernels one launch of the plan runs, and how many pairs use tensor cores. */
 ipb_status ipb_batch_plan_info(const ipb_batch_plan *plan, uint32_t *kernels,
                                uint32_t *tensor_pairs);
+/* The plan's tensor-core launches, in launch order: up to `max` records and
+ * their total count in *count. */
+typedef struct ipb_batch_group {
+    uint32_t row_width; /* tensor-memory row width (8..64 bytes per image row segment) */
+    uint32_t tile_rows; /* output rows per tile */
+    int masked;         /* binary-mask launch */
+    uint32_t pairs;     /* pairs in the launch */
+    uint32_t tiles;     /* tiles the launch's CTAs share */
+} ipb_batch_group;
+ipb_status ipb_batch_plan_groups(const ipb_batch_plan *plan, uint32_t max, ipb_batch_group *out,
+                                 uint32_t *count);
+/* Forget the process's tuning decisions; the next plan re-reads the tuning
+ * file (IPB_TUNING_FILE as it is then). */
+void ipb_batch_tuning_reset(void);
 ipb_status ipb_batch_plan_destroy(ipb_batch_plan *plan);
 
 /* The tensor-core tile plan that a template of w x h pixels (binary mask or
@@ -368,8 +397,16 @@ ipb_status ipb_proposal_net_train_step(ipb_proposal_net *net, const uint8_t *d_s
                                        const int64_t *d_positives, float learning_rate, float *h_loss,
                                        void *stream);
 
+/* The network's features of one image (device, sides non-zero multiples of 4):
+ * d_out receives (height / 4) x 4 x (width / 4) units of 8 bf16 channels, unit
+ * (y, c, x) at index (y * 4 + c) * (width / 4) + x holding channels 8c .. 8c + 7
+ * of position (x, y). kernel 0 runs the 32-channel layers on tcgen05 (the
+ * query path), 1 on mma.sync (the training path); both accumulate in fp32. */
+ipb_status ipb_proposal_net_features(ipb_proposal_net *net, const uint8_t *d_image, uint32_t width,
+                                     uint32_t height, int kernel, void *d_out, void *stream);
+
 typedef struct ipb_propose_options {
-    uint32_t top_k;    /* windows of 32 x 32 positions verified per template (1..32, default 16) */
+    uint32_t top_k;    /* windows of 32 x 32 positions verified per template (1..16, default 16) */
     float min_margin;  /* heatmap confidence margin below which a template falls back (default 0.1) */
     int certify;       /* 1 (default): certify answers; 0: accept the verified windows' best */
 } ipb_propose_options;
@@ -380,6 +417,8 @@ typedef struct ipb_proposal_result {
     float margin;       /* the heatmap's confidence margin */
     uint32_t path;      /* 0: proposals, verified and certified; 1: fallback (low margin);
                            2: fallback (not certified) */
+    uint32_t uncertified; /* blocks of 4 x 4 positions the certificate could not exclude
+                             outside the proposed windows (verified exactly when at most 512) */
 } ipb_proposal_result;
 
 /* Answers n_templates SumOfSquaredErrors queries of 48 x 48 templates

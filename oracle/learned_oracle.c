@@ -183,10 +183,31 @@ double lo_loss_grad(const lo_params *P, const uint8_t *scenes, int N, int sh, in
         double se = 0.0;
         for (size_t i = 0; i < P_all; ++i) se += exp(zt[i] - mx);
         const double lse = mx + log(se);
-        loss += lse - zt[pos[t]];
+        /* the positive set: the 3 x 3 neighbourhood of pos[t] inside its crop */
+        const size_t pt = (size_t)pos[t], base = pt - pt % plane;
+        const int py = (int)((pt % plane) / ws), px = (int)(pt % ws);
+        double mn = -INFINITY, sn = 0.0;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (py + dy >= 0 && py + dy < hs && px + dx >= 0 && px + dx < ws) {
+                    const double v = zt[base + (size_t)(py + dy) * ws + px + dx];
+                    mn = v > mn ? v : mn;
+                }
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (py + dy >= 0 && py + dy < hs && px + dx >= 0 && px + dx < ws)
+                    sn += exp(zt[base + (size_t)(py + dy) * ws + px + dx] - mn);
+        const double lsen = mn + log(sn);
+        loss += lse - lsen;
         /* reuse z as dz */
-        for (size_t i = 0; i < P_all; ++i) zt[i] = exp(zt[i] - lse) / T;
-        zt[pos[t]] -= 1.0 / T;
+        for (size_t i = 0; i < P_all; ++i) {
+            double d = exp(zt[i] - lse);
+            const size_t k = i / plane;
+            const int y = (int)((i % plane) / ws), x = (int)(i % ws);
+            if (k == pt / plane && y - py <= 1 && py - y <= 1 && x - px <= 1 && px - x <= 1)
+                d -= exp(zt[i] - lsen);
+            zt[i] = d / T;
+        }
     }
     loss /= T;
     if (G) {

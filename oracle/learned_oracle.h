@@ -22,8 +22,9 @@
  * [co][ci][ky][kx]; biases [co].
  *
  * Loss of a batch of T templates against N scene crops (in-batch softmax):
- *   L = (1/T) sum_t ( logsumexp_{n,p} z_t(n, p) - z_t(pos_t) )
- * with pos_t a flat index into the N crops' heatmap positions. Backward
+ *   L = (1/T) sum_t ( logsumexp_{n,p} z_t(n, p) - logsumexp_{p in N_t} z_t(p) )
+ * with pos_t a flat index into the N crops' heatmap positions and N_t its
+ * 3 x 3 neighbourhood inside its crop (a multiple-instance positive). Backward
  * treats R() as the identity (straight-through).
  */
 #ifndef LEARNED_ORACLE_H

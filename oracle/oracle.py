@@ -383,3 +383,25 @@ def learned_loss_grad(params, scenes, templates, positives, bf16=True, alpha=0.1
                           _p(z))
     grads = np.concatenate([np.concatenate([dW[k].reshape(-1), db[k]]) for k in range(5)])
     return (loss, grads, z) if want_logits else (loss, grads)
+
+
+def learned_features(params, images, bf16=True, alpha=0.125):
+    """FP64 trunk features (learned_oracle.c lo_trunk_forward) of n u8 images
+    (n, h, w), sides multiples of 4: an (n, 32, h/4, w/4) array."""
+    L = lib()
+    if not getattr(L, "_lo_fwd_bound", False):
+        L.lo_trunk_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_void_p, C.c_void_p]
+        L.lo_trunk_forward.restype = None
+        L._lo_fwd_bound = True
+    images = np.ascontiguousarray(images, np.uint8)
+    n, h, w = images.shape
+    Ws, bs = _lo_split(params)
+    P = _LoParams()
+    for k in range(5):
+        P.W[k] = Ws[k].ctypes.data
+        P.b[k] = bs[k].ctypes.data
+    P.alpha = alpha
+    F = np.empty((n, 32, h // 4, w // 4), np.float64)
+    L.lo_trunk_forward(C.byref(P), _p(images), n, h, w, int(bf16), _p(F), None)
+    return F

@@ -2,13 +2,14 @@
 bounded waits are made to run out, and the call must report IPB_ERR_TIMEOUT
 while the context stays usable.
 
-The test lowers the per-tile wait budget (ipb_debug_set_pipeline_wait_ns) to
-one nanosecond, far below the time any pipeline hand-off takes, so the first
-wait that is not already satisfied gives up. The kernel then records its
-launch tag in the error word, stops its pipeline, waits (with the full 2 s
-budget) for the tensor-core work it issued, frees its tensor memory and exits;
-nothing faults, traps or spins without a limit. The next call, with the
-default budget, must run on the same context and be exact.
+Two test hooks do it: ipb_debug_stall_pipelines makes the MMA-issuing warp of
+each tensor-core kernel first wait on an mbarrier that nothing arrives at (a
+flag that nothing sets), and ipb_debug_set_pipeline_wait_ns shortens the
+per-tile budget of every bounded wait to 100 us so the test stays short. The
+kernel then records its launch tag in the error word, stops its pipeline,
+waits (with the full 2 s budget) for the tensor-core work it issued, frees its
+tensor memory and exits; nothing faults, traps or spins without a limit. The
+next call, with the hooks off, must run on the same context and be exact.
 """
 
 import numpy as np
@@ -25,11 +26,19 @@ def bits(a):
     return np.ascontiguousarray(a, np.float32).view(np.uint32)
 
 
+BUDGET_NS = 100_000
+
+
+def _stall(L, on):
+    L.ipb_debug_set_pipeline_wait_ns(BUDGET_NS if on else 0)
+    L.ipb_debug_stall_pipelines(1 if on else 0)
+
+
 @pytest.fixture
 def tiny_budget():
     L = _lib.lib()
     yield L
-    L.ipb_debug_set_pipeline_wait_ns(0)  # default budget again, whatever happened
+    _stall(L, False)  # default budget and no stall again, whatever happened
 
 
 def test_single_template_wait_runs_out_then_context_recovers(tiny_budget):
@@ -38,13 +47,13 @@ def test_single_template_wait_runs_out_then_context_recovers(tiny_budget):
     tm.set_precision(tm.Precision.ExactFp64)
     tm.set_path(tm.Path.Auto)
     for masked in (False, True):
-        L.ipb_debug_set_pipeline_wait_ns(1)
+        _stall(L, True)
         with pytest.raises(_lib.DeviceError, match=r"status 9\].*timed out"):
             if masked:
                 tm.match_template_with_mask(image, template, 3, mask)
             else:
                 tm.match_template(image, template, 0)
-        L.ipb_debug_set_pipeline_wait_ns(0)
+        _stall(L, False)
         # tensor memory was freed and the context is usable: two exact calls
         for _ in range(2):
             if masked:
@@ -64,10 +73,10 @@ def test_many_templates_wait_runs_out_then_context_recovers(tiny_budget):
     image, templates, _ = synthetic.value_noise_scene(W=512, H=384, n_templates=130, t=32, seed=9)
     di = torch.from_numpy(image).cuda()
     dt = torch.from_numpy(templates).cuda()
-    L.ipb_debug_set_pipeline_wait_ns(1)
+    _stall(L, True)
     device.match_templates_device(di, dt, 3, extremes=False)  # enqueues; the failure shows at the next sync
     torch.cuda.synchronize()
-    L.ipb_debug_set_pipeline_wait_ns(0)
+    _stall(L, False)
     # the next synchronous call of this thread's context reports the earlier launch's timeout ...
     small, tpl = image[:100, :200].copy(), templates[0]
     with pytest.raises(_lib.DeviceError, match=r"status 9\]"):

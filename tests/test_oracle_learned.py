@@ -64,12 +64,19 @@ def test_oracle_gradients_match_finite_differences(seed):
     assert not bad, bad
 
 
-def test_oracle_logits_peak_where_template_matches():
-    # a template cut from a scene, at a downsampled-aligned offset, scores its
-    # own position higher than a random other with any positive-definite net:
-    # check only that logits are finite and the softmax loss is log(P) at zero weights
+def test_oracle_loss_at_zero_weights():
+    # all logits 0: each template's loss is log(P) - log(|N_t|), N_t the 3 x 3
+    # neighbourhood of its positive clipped to the crop
     scenes, templates, pos = _batch(5, n=3, side=24, t=3)
+    pos[0] = 0  # a corner: a neighbourhood of 4
     params = np.zeros(learned.N_PARAMS)
     loss, grads, z = O.learned_loss_grad(params, scenes, templates, pos, bf16=True, want_logits=True)
     assert np.allclose(z, 0.0)
-    assert abs(loss - np.log(z.shape[1])) < 1e-12
+    hs = ws = 24 // 4
+    sizes = []
+    for p in pos:
+        y, x = (p % (hs * ws)) // ws, p % ws
+        sizes.append((min(y + 1, hs - 1) - max(y - 1, 0) + 1) * (min(x + 1, ws - 1) - max(x - 1, 0) + 1))
+    assert sizes[0] == 4
+    exp = np.mean([np.log(z.shape[1]) - np.log(k) for k in sizes])
+    assert abs(loss - exp) < 1e-12
