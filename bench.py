@@ -422,7 +422,9 @@ def run_side_configs(args, world, rank, local) -> dict:
     pairs = synthetic.uneven_pairs(seed=3 + rank)
     items = [(torch.from_numpy(i).to(dev), torch.from_numpy(t).to(dev), m) for i, t, m in pairs]
     batch = device.Batch(items, extremes=True)
+    t0 = time.perf_counter()
     plan = device.BatchPlan(batch, tm.Precision.ExactFp64)
+    plan_ms = (time.perf_counter() - t0) * 1e3
     info = plan.info()
     for _ in range(3):
         plan.launch(stream)
@@ -435,6 +437,13 @@ def run_side_configs(args, world, rank, local) -> dict:
         "value": world * macs / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_batch": ms,
         "pairs_per_s": world * len(pairs) / (ms / 1e3), "kernels_per_batch": info["kernels"],
         "tensor_core_pairs": info["tensor_pairs"], "graph": True,
+        "launches": [f"{g['pairs']} pairs row width {g['row_width']} tile {g['tile_rows']} rows "
+                     f"({g['tiles']} tiles)" for g in info["launches"]],
+        "plan_ms": plan_ms,
+        "tuning": os.environ.get("IPB_AUTOTUNE", "groups (default)"),
+        "roofline": {"bound": "tensor", "achieved": 2.0 * macs / (ms / 1e3) / 1e12,
+                     "peak": 2.0 * peaks()["bf16_tflops"], "unit": "TOP/s",
+                     "frac": 2.0 * macs / (ms / 1e3) / 1e12 / (2.0 * peaks()["bf16_tflops"])},
     }
     plan.close()
     return res
@@ -442,8 +451,11 @@ def run_side_configs(args, world, rank, local) -> dict:
 
 def _learned_scene(seed: int):
     from imageproc_b200 import synthetic
-    image, templates, _ = synthetic.rect_scene(seed=seed)
-    return image, templates
+    image, templates, locs = synthetic.rect_scene(seed=seed)
+    # templates cut from inside one flat rectangle: their exhaustive answer is a
+    # tie broken by scan order, which no proposal can know; they fall back
+    flat = sum(1 for x, y in locs if image[y:y + templates.shape[1], x:x + templates.shape[2]].std() == 0)
+    return image, templates, flat
 
 
 def run_learned(args, world, rank, local) -> dict:
@@ -470,9 +482,10 @@ def run_learned(args, world, rank, local) -> dict:
     net = learned.ProposalNet.trained()
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     ex_ms = le_ms = 0.0
-    agree = queries = 0
+    agree = queries = flat = 0
     paths = [0, 0, 0]
-    for k, (image, templates) in enumerate(scenes):
+    for k, (image, templates, nflat) in enumerate(scenes):
+        flat += nflat
         di = torch.from_numpy(image).to(dev)
         dt = torch.from_numpy(templates).to(dev)
         if k == 0:  # warm-up of both paths
@@ -510,6 +523,7 @@ def run_learned(args, world, rank, local) -> dict:
                     "api": "ipb_propose_and_match_device (top-16 windows, margin 0.1, certified)"},
         "speedup": le_q / ex_q,
         "agreement": agree / max(queries, 1), "queries": queries,
+        "flat_templates": flat,
         "paths": {"proposed_certified": paths[0], "fallback_low_margin": paths[1],
                   "fallback_not_certified": paths[2]},
     }
@@ -737,6 +751,7 @@ def run_ours(args, world, rank, local):
     d2h = len(VARIANTS) * WO * HO * 4
 
     del batch, plan
+    learned = None if args.no_many else run_learned(args, world, rank, local)
     many = None if args.no_many else run_many(args, world, rank, local)
     side = {} if args.no_many else run_side_configs(args, world, rank, local)
     nxt = None if args.no_many else run_next_rows(args, world, rank, local)
@@ -788,6 +803,18 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": bench_config(),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "queries_per_s": world * len(VARIANTS) * args.steps / (ms / 1e3),
+        "graph_ms_per_step": graph_ms / args.steps,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "learned": learned,
+        "many_templates": many,
+        **side,
+        "kernels": {k: {"launches": v["launches"], "total_ms": v["total_ms"],
+                        "share": v["total_ms"] / total_kernel_ms} for k, v in kernels.items()},
         "arm": {"precision": "exact integer sums, FP64 normalisation",
                 "api": ("ipb_batch_plan_launch: one persistent tcgen05 launch per mask kind "
                         "(4 maps each), run eagerly in the timed region so CUDA events bracket "
@@ -798,17 +825,6 @@ def run_ours(args, world, rank, local):
         "fp64_oracle_error": ("0 ulp: all eight maps of this workload equal the FP64 oracle's bit for "
                               "bit (tests/test_gpu_parity.py::test_blob_scene_1920x1080_template_64_exact); "
                               "the reference arm's line reports the reference's own f32 error"),
-        "queries_per_s": world * len(VARIANTS) * args.steps / (ms / 1e3),
-        "graph_ms_per_step": graph_ms / args.steps,
-        "roofline": roofline,
-        "kernels": {k: {"launches": v["launches"], "total_ms": v["total_ms"],
-                        "share": v["total_ms"] / total_kernel_ms} for k, v in kernels.items()},
-        "cpu_baseline": cpu,
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
-        "clocks": clk.summary(),
-        "many_templates": many,
-        **side,
         "next_rows": nxt,
     }
     print(json.dumps(line), flush=True)
@@ -825,6 +841,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-many", action="store_true", help="skip the many-templates workload")
     ap.add_argument("--only-many", action="store_true", help="run the many-templates workload alone")
+    ap.add_argument("--only-side", action="store_true",
+                    help="run the 512x512 single map and the 256-pair uneven batch alone")
     ap.add_argument("--learned-scenes", type=int, default=16)
     ap.add_argument("--only-learned", action="store_true", help="run the learned-proposal workload alone")
     ap.add_argument("--only-next", action="store_true",
@@ -846,6 +864,10 @@ def main():
             nxt = run_next_rows(args, world, rank, local)
             if rank == 0:
                 print(json.dumps(nxt), flush=True)
+        elif args.only_side:
+            side = run_side_configs(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(side), flush=True)
         elif args.only_many:
             many = run_many(args, world, rank, local)
             if rank == 0:

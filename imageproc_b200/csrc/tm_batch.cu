@@ -9,8 +9,12 @@
 //     reference-order kernel for REFERENCE_F32); the autotuner can time both
 //     on the first pair of each shape class and keep the faster;
 //   * tensor-core pairs are grouped by tensor-memory row width and mask
-//     kind, and each group runs as ONE persistent launch over all its tiles
-//     with find_extremes fused into the epilogue;
+//     kind; the autotuner times each group's launch with its natural row
+//     width or twice it and each tile height, and groups that end on the
+//     same (width, height, mask kind) merge; each runs as ONE persistent
+//     launch over all its tiles with find_extremes fused into the epilogue;
+//   * the extremes keys are armed at creation and re-armed by the finish
+//     kernel, so a launch is the group kernels plus one finish kernel;
 //   * the groups' launches run side by side on two streams, the group with
 //     the longest tiles first, each claiming tiles from its own counter, so
 //     the SMs that one launch leaves idle in its last wave take tiles of the
@@ -27,6 +31,9 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "tm_common.cuh"
 #include "tm_internal.h"
@@ -73,9 +80,17 @@ namespace ipb {
 namespace {
 
 // ---- autotuner -----------------------------------------------------------------
-// Shape class of a pair: (w, h, masked, normalised). The decision is cached
-// per process and, when IPB_TUNING_FILE names a file, persisted across runs
-// ("w h masked norm tensor" per line).
+// Two decisions are tuned and cached per process, and persisted in a text file
+// (IPB_TUNING_FILE, default ~/.cache/imageproc_b200/tuning.txt; an empty
+// IPB_TUNING_FILE keeps them in memory only):
+//  * per batch group (on unless IPB_AUTOTUNE=0): the tensor-memory row width
+//    (the group's natural width or twice it) and the tile height, timed on
+//    the group's own pairs; key = (natural width, masked, tallest template
+//    rounded up to 8, log2 of the group's output positions, log2 of its
+//    largest image side). Line: "group ks0 masked h8 wlog mlog ks nt".
+//  * per pair shape class (IPB_AUTOTUNE=1): tensor cores or the CUDA-core
+//    kernel, timed on the first pair of each (w, h, masked, normalised).
+//    Line: "pair w h masked norm tensor".
 struct TuneKey {
   uint32_t w, h;
   int masked, norm;
@@ -83,28 +98,88 @@ struct TuneKey {
     return std::tie(w, h, masked, norm) < std::tie(o.w, o.h, o.masked, o.norm);
   }
 };
+struct GroupKey {
+  uint32_t ks0;
+  int masked;
+  uint32_t h8, wlog, mlog;
+  bool operator<(const GroupKey& o) const {
+    return std::tie(ks0, masked, h8, wlog, mlog) < std::tie(o.ks0, o.masked, o.h8, o.wlog, o.mlog);
+  }
+};
+struct GroupChoice {
+  uint32_t ks, nt;
+};
 std::mutex g_tune_mu;
 std::map<TuneKey, bool> g_tune;
+std::map<GroupKey, GroupChoice> g_group_tune;
 bool g_tune_loaded = false;
+
+std::string tuning_file() {
+  const char* f = std::getenv("IPB_TUNING_FILE");
+  if (f) return f;
+  const char* home = std::getenv("HOME");
+  if (!home || !*home) return "";
+  const std::string dir = std::string(home) + "/.cache/imageproc_b200";
+  mkdir((std::string(home) + "/.cache").c_str(), 0755);
+  mkdir(dir.c_str(), 0755);
+  return dir + "/tuning.txt";
+}
 
 void tune_load_locked() {
   if (g_tune_loaded) return;
   g_tune_loaded = true;
-  const char* f = std::getenv("IPB_TUNING_FILE");
-  if (!f) return;
+  const std::string f = tuning_file();
+  if (f.empty()) return;
   std::ifstream in(f);
-  TuneKey k;
-  int t;
-  while (in >> k.w >> k.h >> k.masked >> k.norm >> t) g_tune[k] = t != 0;
+  std::string line;
+  while (std::getline(in, line)) {
+    std::istringstream ls(line);
+    std::string kind;
+    ls >> kind;
+    if (kind == "pair") {
+      TuneKey k;
+      int t;
+      if (ls >> k.w >> k.h >> k.masked >> k.norm >> t) g_tune[k] = t != 0;
+    } else if (kind == "group") {
+      GroupKey k;
+      GroupChoice c;
+      if (ls >> k.ks0 >> k.masked >> k.h8 >> k.wlog >> k.mlog >> c.ks >> c.nt) g_group_tune[k] = c;
+    }
+  }
 }
 
 void tune_store_locked() {
-  const char* f = std::getenv("IPB_TUNING_FILE");
-  if (!f) return;
-  std::ofstream out(f);
-  for (auto& kv : g_tune)
-    out << kv.first.w << ' ' << kv.first.h << ' ' << kv.first.masked << ' ' << kv.first.norm << ' '
-        << (kv.second ? 1 : 0) << '\n';
+  const std::string f = tuning_file();
+  if (f.empty()) return;
+  const std::string tmp = f + ".tmp" + std::to_string((long)getpid());
+  {
+    std::ofstream out(tmp);
+    for (auto& kv : g_tune)
+      out << "pair " << kv.first.w << ' ' << kv.first.h << ' ' << kv.first.masked << ' ' << kv.first.norm << ' '
+          << (kv.second ? 1 : 0) << '\n';
+    for (auto& kv : g_group_tune)
+      out << "group " << kv.first.ks0 << ' ' << kv.first.masked << ' ' << kv.first.h8 << ' ' << kv.first.wlog
+          << ' ' << kv.first.mlog << ' ' << kv.second.ks << ' ' << kv.second.nt << '\n';
+    if (!out) return;
+  }
+  std::rename(tmp.c_str(), f.c_str());  // whole files only, for processes sharing the file
+}
+
+int autotune_mode() {  // 0: off, 1: groups, 2: groups and per-pair paths
+  const char* v = std::getenv("IPB_AUTOTUNE");
+  if (!v) return 1;
+  if (std::strcmp(v, "0") == 0) return 0;
+  if (std::strcmp(v, "1") == 0) return 2;
+  return 1;
+}
+
+uint32_t floor_log2(double v) {
+  uint32_t l = 0;
+  while (v >= 2.0) {
+    v *= 0.5;
+    ++l;
+  }
+  return l;
 }
 
 // Cost model: tensor cores whenever the shape is supported (they win from
@@ -165,6 +240,72 @@ ipb_status to_status(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return to_status(e_, what); \
   } while (0)
 
+// Times a natural group's launch with each candidate (row width ks0 or
+// 2 ks0, each tile height) on the group's own pairs and returns the fastest.
+// The timing launches write the pairs' outputs and extremes keys; the
+// caller re-arms the keys afterwards.
+template <class KeysOf>
+ipb_status tune_group(ipb_batch_plan* p, const std::vector<uint32_t>& mem, uint32_t ks0, bool masked, uint32_t hmax,
+                      KeysOf keys_of, GroupChoice& best) {
+  best = GroupChoice{ks0, 0};
+  uint32_t nts[2];
+  const uint32_t nnt = umma_tile_heights(masked, nts);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  IPB_TRY(cudaEventCreate(&e0), "event");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return to_status(cudaErrorMemoryAllocation, "event");
+  }
+  float best_ms = 1e30f;
+  cudaError_t err = cudaSuccess;
+  for (uint32_t ks : {ks0, 2 * ks0}) {
+    for (uint32_t t = 0; t < nnt && err == cudaSuccess; ++t) {
+      UmmaPlan pl;
+      if (!umma_plan_for(ks, masked, hmax, pl, nts[t])) continue;
+      std::vector<UmmaProblem> probs;
+      uint32_t tiles = 0;
+      for (uint32_t i : mem) {
+        probs.push_back(umma_problem(p->args[i], pl, tiles, keys_of(i)));
+        tiles += umma_problem_tiles(probs.back(), pl);
+      }
+      UmmaLaunch L{};
+      UmmaProblem* d_probs = nullptr;
+      if (probs.size() > kInlineProblems) {
+        if ((err = cudaMalloc(&d_probs, sizeof(UmmaProblem) * probs.size())) != cudaSuccess) break;
+        cudaMemcpy(d_probs, probs.data(), sizeof(UmmaProblem) * probs.size(), cudaMemcpyHostToDevice);
+      } else {
+        for (size_t i = 0; i < probs.size(); ++i) L.inl[i] = probs[i];
+      }
+      L.probs = d_probs;
+      L.nprobs = (uint32_t)probs.size();
+      L.tiles = tiles;
+      L.err = p->d_err;
+      L.tag = p->tag;
+      L.wait_ns = pipeline_wait_ns();
+      L.stall = 0u;
+      L.sched = p->d_sched;
+      float ms_best = 1e30f;
+      for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {  // the first launch is a warm-up
+        cudaEventRecord(e0, nullptr);
+        err = launch_umma_batch(pl, L, nullptr, nullptr);
+        cudaEventRecord(e1, nullptr);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (err == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+          ms_best = std::min(ms_best, ms);
+      }
+      if (d_probs) cudaFree(d_probs);
+      if (err == cudaSuccess && ms_best < best_ms) {
+        best_ms = ms_best;
+        best = GroupChoice{ks, nts[t]};
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return to_status(err, "tuning launch");
+}
+
 void release(ipb_batch_plan* p) {
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
@@ -181,11 +322,7 @@ void release(ipb_batch_plan* p) {
 // Enqueue the plan's launch sequence (used once under stream capture, and
 // directly when profiling so each kernel can be timed).
 ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kernels) {
-  uint32_t k = 0;
-  if (p->nkeys) {
-    IPB_TRY(launch_extremes_keys_init(p->d_keys, p->nkeys, s), "extremes init");
-    ++k;
-  }
+  uint32_t k = 0;  // the keys were armed at creation and are re-armed by the finish kernel
   // groups after the first run on the side stream, between a fork and a join
   // on s; concurrent launches are timed as one span on s
   const bool side_by_side = p->groups.size() >= 2 && p->side;
@@ -213,6 +350,7 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     L.err = p->d_err;
     L.tag = p->tag;
     L.wait_ns = pipeline_wait_ns();
+    L.stall = pipeline_stall() ? 1u : 0u;
     L.sched = p->d_sched + 2 * gi;
     KernelTimer* t = timed && !side_by_side ? acquire_kernel_timer() : nullptr;
     launch_err = launch_umma_batch(g.plan, L, gs, t);
@@ -318,18 +456,17 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
     return fail(to_status(e, "cudaMalloc"));
 
   // kernel family per pair, then tensor groups keyed by (row width, masked)
-  const bool autotune = std::getenv("IPB_AUTOTUNE") && std::strcmp(std::getenv("IPB_AUTOTUNE"), "1") == 0;
+  const int tune = autotune_mode();
   std::map<uint32_t, std::vector<uint32_t>> by_key;
   for (uint32_t i = 0; i < n; ++i) {
     MatchArgs a = p->args[i];
     if (!a.w || !a.h) continue;
     a.stream = nullptr;
-    if (choose_tensor(a, autotune, p->d_scratch, p->d_err)) {
+    if (choose_tensor(a, tune == 2, p->d_scratch, p->d_err)) {
       p->tensor[i] = true;
       by_key[umma_group_key(a)].push_back(i);
     }
   }
-  std::vector<unsigned long long> keys_host;
   std::vector<uint32_t> widths;
   std::vector<ipb_extremes_f32*> outs;
   // one key slot per tensor pair with an extremes record
@@ -349,18 +486,72 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
     cudaMemcpy(p->d_widths, widths.data(), sizeof(uint32_t) * p->nkeys, cudaMemcpyHostToDevice);
     cudaMemcpy(p->d_outs, outs.data(), sizeof(void*) * p->nkeys, cudaMemcpyHostToDevice);
   }
+  if ((e = umma_prepare_kernels()) != cudaSuccess) return fail(to_status(e, "kernel attributes"));
+  if (!by_key.empty()) {
+    // tile counters: two words per launch, reset by each launch's last CTA
+    const size_t sched_bytes = sizeof(unsigned int) * 2 * by_key.size();
+    if ((e = cudaMalloc(&p->d_sched, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMalloc"));
+    if ((e = cudaMemset(p->d_sched, 0, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
+  }
+  auto keys_of = [&](uint32_t i) { return slot[i] >= 0 ? p->d_keys + 2 * slot[i] : nullptr; };
+  // each natural group's (row width, tile height): tuned, or the natural
+  // width with the tallest tiles; groups that land on the same (width,
+  // height, mask kind) share one launch
+  std::map<std::tuple<bool, uint32_t, uint32_t>, std::vector<uint32_t>> launches;
   for (auto& kv : by_key) {
+    const std::vector<uint32_t>& mem = kv.second;
+    const bool masked = p->args[mem.front()].mask != nullptr;
+    const uint32_t ks0 = kv.first / 2;  // umma_group_key = row width * 2 + masked
+    GroupChoice c{ks0, 0};
+    if (tune) {
+      uint32_t hmax = 0, side = 0;
+      double pos = 0;
+      for (uint32_t i : mem) {
+        const MatchArgs& a = p->args[i];
+        hmax = std::max(hmax, a.h);
+        side = std::max(side, std::max(a.W, a.H));
+        pos += (double)(a.W - a.w + 1) * (a.H - a.h + 1);
+      }
+      const GroupKey gk{ks0, masked ? 1 : 0, (hmax + 7) & ~7u, floor_log2(pos), floor_log2(side)};
+      bool have = false;
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_load_locked();
+        auto it = g_group_tune.find(gk);
+        if (it != g_group_tune.end()) {
+          c = it->second;
+          have = true;
+        }
+      }
+      if (!have) {
+        ipb_status st = tune_group(p, mem, ks0, masked, hmax, keys_of, c);
+        if (st != IPB_OK) return fail(st);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_group_tune[gk] = c;
+        tune_store_locked();
+      }
+    }
+    auto& dst = launches[std::make_tuple(masked, c.ks, c.nt)];
+    dst.insert(dst.end(), mem.begin(), mem.end());
+  }
+  for (auto& kv : launches) {
     ipb_batch_plan::Group g;
-    uint32_t hmax = 0;
-    for (uint32_t i : kv.second) hmax = std::max(hmax, p->args[i].h);
-    const MatchArgs& a0 = p->args[kv.second.front()];
-    uint32_t ks = 8;
-    while (ks * 4 < ((a0.w + 31) & ~31u)) ks *= 2;
-    if (!umma_plan_for(ks, a0.mask != nullptr, hmax, g.plan)) return fail((ipb_status)report_error(IPB_ERR_CUDA, "no tensor-core plan"));
+    const bool masked = std::get<0>(kv.first);
+    uint32_t ks = std::get<1>(kv.first);
+    const uint32_t nt = std::get<2>(kv.first);
     g.members = kv.second;
+    std::sort(g.members.begin(), g.members.end());
+    uint32_t hmax = 0;
+    for (uint32_t i : g.members) {
+      hmax = std::max(hmax, p->args[i].h);
+      ks = std::max(ks, umma_row_width(p->args[i].w));
+    }
+    // a cached choice that no longer fits falls back to the tallest tiles
+    if (!umma_plan_for(ks, masked, hmax, g.plan, nt) && !umma_plan_for(ks, masked, hmax, g.plan, 0))
+      return fail((ipb_status)report_error(IPB_ERR_CUDA, "no tensor-core plan"));
     uint32_t tiles = 0;
     for (uint32_t i : g.members) {
-      UmmaProblem q = umma_problem(p->args[i], g.plan, tiles, slot[i] >= 0 ? p->d_keys + 2 * slot[i] : nullptr);
+      UmmaProblem q = umma_problem(p->args[i], g.plan, tiles, keys_of(i));
       tiles += umma_problem_tiles(q, g.plan);
       g.probs.push_back(q);
     }
@@ -372,6 +563,11 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
     }
     p->groups.push_back(std::move(g));
   }
+  // arm the extremes keys (after any tuning launches) and clear the error word
+  if (p->nkeys && ((e = launch_extremes_keys_init(p->d_keys, p->nkeys, nullptr)) != cudaSuccess ||
+                   (e = cudaStreamSynchronize(nullptr)) != cudaSuccess))
+    return fail(to_status(e, "extremes keys"));
+  if ((e = cudaMemset(p->d_err, 0, sizeof(unsigned int))) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
   // longest tiles first (binary masks: three correlations per row; then the
   // widest rows), so that the launch started second fills the tail of the first
   std::stable_sort(p->groups.begin(), p->groups.end(),
@@ -379,18 +575,12 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
                      if (x.plan.masked != y.plan.masked) return x.plan.masked;
                      return x.plan.ks > y.plan.ks;
                    });
-  if (!p->groups.empty()) {
-    const size_t sched_bytes = sizeof(unsigned int) * 2 * p->groups.size();
-    if ((e = cudaMalloc(&p->d_sched, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMalloc"));
-    if ((e = cudaMemset(p->d_sched, 0, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
-  }
   if (p->groups.size() >= 2) {
     if ((e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess)
       return fail(to_status(e, "side stream"));
   }
-  if ((e = umma_prepare_kernels()) != cudaSuccess) return fail(to_status(e, "kernel attributes"));
   uint32_t kernels = 0;
   if (capture) {
     // capture the launch sequence once
@@ -442,6 +632,25 @@ IPB_API ipb_status ipb_batch_plan_info(const ipb_batch_plan* plan, uint32_t* ker
   if (!plan) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null plan");
   if (kernels) *kernels = plan->kernels;
   if (tensor_pairs) *tensor_pairs = (uint32_t)std::count(plan->tensor.begin(), plan->tensor.end(), true);
+  return IPB_OK;
+}
+
+IPB_API void ipb_batch_tuning_reset(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
+  g_group_tune.clear();
+  g_tune_loaded = false;
+}
+
+IPB_API ipb_status ipb_batch_plan_groups(const ipb_batch_plan* plan, uint32_t max, ipb_batch_group* out,
+                                         uint32_t* count) {
+  if (!plan || (max && !out)) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  const uint32_t n = (uint32_t)plan->groups.size();
+  for (uint32_t i = 0; i < n && i < max; ++i) {
+    const ipb_batch_plan::Group& g = plan->groups[i];
+    out[i] = ipb_batch_group{g.plan.ks, g.plan.NT, g.plan.masked ? 1 : 0, (uint32_t)g.members.size(), g.tiles};
+  }
+  if (count) *count = n;
   return IPB_OK;
 }
 

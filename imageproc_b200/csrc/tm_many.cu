@@ -33,6 +33,8 @@
 // fold them into per-template extremes. Scores are position-major:
 // out[(y * Wo + x) * n_templates + t].
 // Every wait is bounded (2 s) and reports through the error word.
+#include <type_traits>
+
 #include "tm_common.cuh"
 #include "tm_internal.h"
 #include "tm_sm100.cuh"
@@ -73,6 +75,7 @@ struct ManyParams {
   unsigned int* err;
   unsigned int tag;
   unsigned long long wait_ns;  // budget of the bounded waits per tile (pipeline_wait_ns())
+  uint32_t stall;              // pipeline_stall() at launch
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
@@ -111,7 +114,9 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
   const ManyParams& p = *c.p;
   const uint32_t q = (c.e + kBuildWarps) & 3;  // = warp & 3, the lanes this warp may access
   if constexpr (kTplM) {
-    // lanes are templates; this warp takes kPosW of the tile's 128 positions
+    // lanes are templates; this warp takes kPosW (= 32) of the tile's 128
+    // positions, as two halves of 16 (one tensor-memory load each)
+    static_assert(kPosW == 32, "two halves of 16 positions per strip");
     const uint32_t mb = (c.e >> 2) * kPosW;
     const uint32_t tl = q * 32 + c.lane;
     const bool t_ok = tl < c.nt;
@@ -123,6 +128,9 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
     const double rT = (kNormW && tss) ? rsqrt_u32(tss) : 0.0;
     const int mvalid = (int)p.Ho - (int)(c.y0 + mb);  // positions of the share inside the map
     const size_t rstride = (size_t)p.Wo * p.n;
+    auto score_of = [&](uint32_t v, uint32_t y) -> uint32_t {
+      return method_is_sse(kMethod) ? (y + tss - 2u * v) : v;
+    };
     for (uint32_t xi = 0; xi < c.nx; ++xi) {
       const uint32_t g = c.gx + xi, d = g & 1u;
       if (!__all_sync(0xffffffffu, mbar_wait_sleep(&c.dfull[d], (g >> 1) & 1u, c.deadline))) return false;
@@ -130,69 +138,117 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
       const uint32_t x = c.x0 + xi;
       const uint32_t* ycol = c.s_y + xi * kM + mb;
       float* ocol = (p.out && t_ok) ? p.out + ((size_t)(c.y0 + mb) * p.Wo + x) * p.n + c.t0 + tl : nullptr;
-      const uint32_t idx0 = (c.y0 + mb) * p.Wo + x;
+      // a zero norm anywhere in the share (a window of zeros, or this lane's
+      // template all zeros) sends the strip through the general quotient
+      bool general = false;
       if constexpr (kNormW) {
         __syncwarp();
-        for (uint32_t i = c.lane; i < (uint32_t)kPosW; i += 32) {
-          const uint32_t yv = ycol[i];
-          s_ryw[i] = yv ? rsqrt_u32(yv) : 0.0;
-        }
+        const uint32_t yv = ycol[c.lane];
+        s_ryw[c.lane] = yv ? rsqrt_u32(yv) : 0.0;
+        general = __any_sync(0xffffffffu, yv == 0u) || rT == 0.0;
         __syncwarp();
       }
-      // extremes of this strip: scores are never negative, so their f32 bits
-      // order like the values; positions come in increasing index order, so
-      // strict comparisons keep the first occurrence
-      uint32_t bmn = 0xFFFFFFFFu, jmn = 0, bmx = 0, jmx = 0;
-      for (int cc = 0; cc < kPosW; cc += 16) {
-        uint32_t v[16];
-        tmem_ld16(tmem_addr(c.tmem, q * 32, d * 128 + mb + cc), v);
-        uint32_t Y[16];
 #pragma unroll
-        for (int k = 0; k < 16; k += 4) {
-          const uint4 y4 = *reinterpret_cast<const uint4*>(ycol + cc + k);
-          Y[k] = y4.x;
-          Y[k + 1] = y4.y;
-          Y[k + 2] = y4.z;
-          Y[k + 3] = y4.w;
-        }
-        tmem_wait_ld();
-        auto one = [&](int k) {
-          float f;
-          if constexpr (kNormW) {
-            const uint32_t score = method_is_sse(kMethod) ? (Y[k] + tss - 2u * v[k]) : v[k];
-            f = norm_quotient_fp64_w(score, __dmul_rn(s_ryw[cc + k], rT), Y[k], tss);
-          } else {
-            f = finish_score32(kMethod, kPrec, v[k], Y[k], tss);
+      for (int half = 0; half < 32; half += 16) {
+        if (half >= mvalid) break;  // warp-uniform: past the map's last row
+        const int nv = min(16, mvalid - half);
+        const uint32_t taddr = tmem_addr(c.tmem, q * 32, d * 128 + mb + half);
+        float* o = ocol ? ocol + (size_t)half * rstride : nullptr;
+        // Fast pass: each value is scored branch-free, stored at once and
+        // folded into the half's smallest and largest bits (scores are never
+        // negative, so f32 bits order like the values), keeping few values
+        // live. FP64 quotients near an f32 rounding midpoint are flagged.
+        uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+        bool undecided = false;
+        {
+          uint32_t v[16], Y[16];
+          tmem_ld16(taddr, v);
+#pragma unroll
+          for (int k = 0; k < 16; k += 4) {
+            const uint4 y4 = *reinterpret_cast<const uint4*>(ycol + half + k);
+            Y[k] = y4.x;
+            Y[k + 1] = y4.y;
+            Y[k + 2] = y4.z;
+            Y[k + 3] = y4.w;
           }
-          if (ocol) ocol[(size_t)(cc + k) * rstride] = f;
-          if constexpr (kExt) {
-            const uint32_t b = __float_as_uint(f);
-            if (b < bmn) {
-              bmn = b;
-              jmn = cc + k;
+          tmem_wait_ld();
+          auto pass = [&](auto full_tag) {
+            constexpr bool kFull = decltype(full_tag)::value;
+#pragma unroll
+            for (int k = 0; k < 16; k += 2) {
+              uint32_t b0, b1;
+              if constexpr (kNormW) {
+                const double2 r2 = *reinterpret_cast<const double2*>(s_ryw + half + k);
+                b0 = norm_bits_fp64_fast(score_of(v[k], Y[k]), __dmul_rn(r2.x, rT), undecided);
+                b1 = norm_bits_fp64_fast(score_of(v[k + 1], Y[k + 1]), __dmul_rn(r2.y, rT), undecided);
+              } else {
+                b0 = __float_as_uint(finish_score32(kMethod, kPrec, v[k], Y[k], tss));
+                b1 = __float_as_uint(finish_score32(kMethod, kPrec, v[k + 1], Y[k + 1], tss));
+              }
+              if (kFull || k < nv) {
+                if (o) o[(size_t)k * rstride] = __uint_as_float(b0);
+                mn = min(mn, b0);
+                mx = max(mx, b0);
+              }
+              if (kFull || k + 1 < nv) {
+                if (o) o[(size_t)(k + 1) * rstride] = __uint_as_float(b1);
+                mn = min(mn, b1);
+                mx = max(mx, b1);
+              }
             }
-            if (b > bmx) {
-              bmx = b;
-              jmx = cc + k;
+          };
+          if (nv == 16)
+            pass(std::true_type{});
+          else
+            pass(std::false_type{});
+        }
+        // Second pass, rare and warp-uniform: a half with a flagged or
+        // zero-norm quotient (re-stored through the general quotient), or
+        // whose extremes could beat this lane's running keys (the keys with
+        // the half's first index bound what the half can contribute). The
+        // sums are reloaded and the first occurrence of each extreme found.
+        const uint32_t idx0 = (c.y0 + mb + half) * p.Wo + x;
+        const bool want_ext =
+            kExt && t_ok &&
+            ((((unsigned long long)(mn | 0x80000000u) << 32) | idx0) < c.kmin ||
+             (((unsigned long long)(mx | 0x80000000u) << 32) | (0xFFFFFFFFu - idx0)) > c.kmax);
+        const bool fix = general || undecided;
+        if (__any_sync(0xffffffffu, fix || want_ext)) {
+          uint32_t v[16];
+          tmem_ld16(taddr, v);
+          tmem_wait_ld();
+          uint32_t bmn = 0xFFFFFFFFu, jmn = 0, bmx = 0u, jmx = 0;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            if (k >= nv) break;
+            const uint32_t yk = ycol[half + k];
+            const uint32_t s = score_of(v[k], yk);
+            uint32_t bk;
+            if constexpr (kNormW) {
+              const double w = __dmul_rn(s_ryw[half + k], rT);
+              bool u = general;
+              bk = general ? 0u : norm_bits_fp64_fast(s, w, u);
+              if (u) {
+                bk = __float_as_uint(norm_quotient_fp64_w(s, w, yk, tss));
+                if (o) o[(size_t)k * rstride] = __uint_as_float(bk);
+              }
+            } else {
+              bk = __float_as_uint(finish_score32(kMethod, kPrec, v[k], yk, tss));
+            }
+            if (bk < bmn) {
+              bmn = bk;
+              jmn = k;
+            }
+            if (bk > bmx) {
+              bmx = bk;
+              jmx = k;
             }
           }
-        };
-        if (cc + 16 <= mvalid) {
-#pragma unroll
-          for (int k = 0; k < 16; ++k) one(k);
-        } else {
-#pragma unroll
-          for (int k = 0; k < 16; ++k)
-            if (cc + k < mvalid) one(k);
-        }
-      }
-      if constexpr (kExt) {
-        // fold into the running keys (order_key of a non-negative f32 is its
-        // bits with the sign bit set); ties across strips go to the lower index
-        if (t_ok && mvalid > 0) {
-          const uint32_t imn = idx0 + jmn * p.Wo, imx = idx0 + jmx * p.Wo;
-          c.kmin = min(c.kmin, ((unsigned long long)(bmn | 0x80000000u) << 32) | imn);
-          c.kmax = max(c.kmax, ((unsigned long long)(bmx | 0x80000000u) << 32) | (0xFFFFFFFFu - imx));
+          if (kExt && t_ok) {
+            c.kmin = min(c.kmin, ((unsigned long long)(bmn | 0x80000000u) << 32) | (idx0 + jmn * p.Wo));
+            c.kmax = max(c.kmax,
+                         ((unsigned long long)(bmx | 0x80000000u) << 32) | (0xFFFFFFFFu - (idx0 + jmx * p.Wo)));
+          }
         }
       }
       tc_fence_before();
@@ -267,31 +323,10 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
   }
 }
 
-template <bool kTplM, int kMethod>
-__device__ __forceinline__ bool epilogue_m(EpiCtx& c, bool fp64, bool ext) {
-  if constexpr (!method_is_norm(kMethod)) fp64 = true;  // precision only affects the normalisation
-  if (fp64)
-    return ext ? epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, true>(c)
-               : epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, false>(c);
-  return ext ? epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_F32, true>(c)
-             : epilogue<kTplM, kMethod, IPB_PRECISION_EXACT_F32, false>(c);
-}
-
-template <bool kTplM>
-__device__ __forceinline__ bool epilogue_dispatch(EpiCtx& c, int method, bool fp64, bool ext) {
-  switch (method) {
-    case kSse:
-      return epilogue_m<kTplM, kSse>(c, fp64, ext);
-    case kSseNorm:
-      return epilogue_m<kTplM, kSseNorm>(c, fp64, ext);
-    case kCcorr:
-      return epilogue_m<kTplM, kCcorr>(c, fp64, ext);
-    default:
-      return epilogue_m<kTplM, kCcorrNorm>(c, fp64, ext);
-  }
-}
-
-template <bool kTplM>
+// One kernel per (operand assignment, method, precision, extremes): each
+// gets its own register allocation for its epilogue. Precision only affects
+// the normalised methods; the others use EXACT_FP64's instance.
+template <bool kTplM, int kMethod, int kPrec, bool kExt>
 __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_constant__ ManyParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* sfull = reinterpret_cast<uint64_t*>(smem);   // [kStrips] strip built
@@ -367,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
   const uint32_t idesc = kTplM ? idesc_u8u8_s32(128, kM) : idesc_u8u8_s32(kM, p.NB);
-  const bool do_ext = p.ext != nullptr;
+  constexpr bool do_ext = kExt;
   // templates as M: this lane's template and its running extremes keys
   const uint32_t tl = ((uint32_t)warp & 3u) * 32 + lane;
   const bool t_ok = tl < nt;
@@ -464,7 +499,9 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
       const uint32_t sstep = lbo_s >> 4, tstep = lbo_t >> 4;
       const uint64_t tdesc0 = smem_desc_noswizzle(smem_u32(bmat), lbo_t, 128);
       const uint32_t nk = p.kw / 32;
-      for (uint32_t xi = 0; xi < nx; ++xi) {
+      // test hook: a wait on the drain barrier, which nothing arrives at before the end
+      if (p.stall && !__all_sync(0xffffffffu, mbar_wait(drain, 0, deadline))) ok = false;
+      for (uint32_t xi = 0; ok && xi < nx; ++xi) {
         const uint32_t g = gx + xi, s = g % kStrips, d = g & 1u;
         const bool got_s = mbar_wait(&sfull[s], (g / kStrips) & 1u, deadline);
         const bool got_d = got_s && (g < 2 || mbar_wait(&dempty[d], ((g >> 1) + 1) & 1u, deadline));
@@ -506,7 +543,7 @@ __global__ void __launch_bounds__(kThreads, 1) many_match_kernel(const __grid_co
       EpiCtx c{&p, tmem, dfull, dempty, s_y, s_tss, s_ext, reinterpret_cast<double*>(smem + p.ry_off),
                gx, nx, x0, y0, t0, nt,
                (uint32_t)(warp - kBuildWarps), (uint32_t)lane, deadline, kmin, kmax};
-      ok = epilogue_dispatch<kTplM>(c, p.method, p.precision == IPB_PRECISION_EXACT_FP64, do_ext);
+      ok = epilogue<kTplM, kMethod, kPrec, kExt>(c);
       kmin = c.kmin;
       kmax = c.kmax;
       if (!ok) {
@@ -590,6 +627,35 @@ uint32_t many_carve(ManyParams& p, uint32_t nb) {
 
 constexpr uint32_t kSmemLimit = 227u * 1024u;
 
+using ManyKernel = void (*)(ManyParams);
+
+template <bool kTplM, int kMethod>
+ManyKernel many_kernel_m(bool fp64, bool ext) {
+  if (!method_is_norm(kMethod) || fp64)
+    return ext ? many_match_kernel<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, true>
+               : many_match_kernel<kTplM, kMethod, IPB_PRECISION_EXACT_FP64, false>;
+  return ext ? many_match_kernel<kTplM, kMethod, IPB_PRECISION_EXACT_F32, true>
+             : many_match_kernel<kTplM, kMethod, IPB_PRECISION_EXACT_F32, false>;
+}
+
+template <bool kTplM>
+ManyKernel many_kernel_a(int method, bool fp64, bool ext) {
+  switch (method) {
+    case kSse:
+      return many_kernel_m<kTplM, kSse>(fp64, ext);
+    case kSseNorm:
+      return many_kernel_m<kTplM, kSseNorm>(fp64, ext);
+    case kCcorr:
+      return many_kernel_m<kTplM, kCcorr>(fp64, ext);
+    default:
+      return many_kernel_m<kTplM, kCcorrNorm>(fp64, ext);
+  }
+}
+
+ManyKernel many_kernel_for(bool tplm, int method, bool fp64, bool ext) {
+  return tplm ? many_kernel_a<true>(method, fp64, ext) : many_kernel_a<false>(method, fp64, ext);
+}
+
 }  // namespace
 
 cudaError_t launch_many_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s) {
@@ -649,13 +715,16 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   p.err = err;
   p.tag = tag;
   p.wait_ns = pipeline_wait_ns();
+  p.stall = pipeline_stall() ? 1u : 0u;
   static PerDeviceOnce attr;
   cudaError_t e = attr.run([] {
-    cudaError_t r = cudaFuncSetAttribute(many_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kSmemLimit);
-    if (r == cudaSuccess)
-      r = cudaFuncSetAttribute(many_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSmemLimit);
+    cudaError_t r = cudaSuccess;
+    for (int a = 0; a < 2 && r == cudaSuccess; ++a)
+      for (int m = 0; m < 4 && r == cudaSuccess; ++m)
+        for (int f = 0; f < 2 && r == cudaSuccess; ++f)
+          for (int x = 0; x < 2 && r == cudaSuccess; ++x)
+            r = cudaFuncSetAttribute(many_kernel_for(a != 0, m, f != 0, x != 0),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemLimit);
     return r;
   });
   if (e != cudaSuccess) return e;
@@ -665,10 +734,8 @@ cudaError_t launch_many(const uint8_t* img, uint32_t W, uint32_t H, const uint8_
   if (per > p.spatial) per = p.spatial;
   const uint32_t grid = per * p.nblocks;
   timer_begin(timer, kKernelMany, stream);
-  if (tplm)
-    many_match_kernel<true><<<grid, kThreads, smem, stream>>>(p);
-  else
-    many_match_kernel<false><<<grid, kThreads, smem, stream>>>(p);
+  many_kernel_for(tplm, method, precision == IPB_PRECISION_EXACT_FP64, ext_keys != nullptr)
+      <<<grid, kThreads, smem, stream>>>(p);
   count_launch(kKernelMany);
   timer_end(timer, stream);
   return cudaGetLastError();

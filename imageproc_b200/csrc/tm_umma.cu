@@ -23,7 +23,10 @@
 // Both parts of I^2 = 255 floor(I^2/255) + I^2 mod 255 lie in 0..255, and
 // 255*m is a u8 for a binary mask, so the two u8 x u8 correlations sum to
 // Y = sum I^2 m in one accumulator, exactly: every partial sum is at most
-// 65025 * 16384 < 2^31 for the masked template sizes taken here.
+// 65025 * 16384 < 2^31 for the masked template sizes taken here. Masked
+// CrossCorrelation needs X alone (the reference's masked score is
+// sum I T m^2, src/template_matching.rs:336-351): its problems skip the
+// I^2 planes and correlations 1 and 2.
 // B_r is a window of one buffer Z_c (Q_c with its rows reversed and 16 zero
 // rows on each side) stored in the canonical no-swizzle K-major layout, whose
 // rows are 16 bytes apart: moving from r to r+1 moves B's start address by
@@ -195,7 +198,10 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
     uint32_t vx[16];
     tmem_ld16(tmem_addr(e.tmem, e.lane_base, n0), vx);
     uint32_t yv[16];
-    if constexpr (MASKED) {
+    if constexpr (MASKED && kMethod == kCcorr) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) yv[k] = 0u;  // not computed: CrossCorrelation is X alone
+    } else if constexpr (MASKED) {
       tmem_ld16(tmem_addr(e.tmem, e.lane_base, e.NT + n0), yv);
     } else {
       // window sums of the chunk: loads first, then the sliding chain
@@ -411,7 +417,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       z_h = q.h;
       z_kmma = q.kmma;
     }
-    if constexpr (MASKED) {
+    // masked CrossCorrelation scores X alone: no Y correlations, no I^2 planes
+    const bool need_y = !MASKED || q.method != kCcorr;
+    if (MASKED && need_y) {
       // the two u8 parts of I^2 (I^2 mod 255, floor(I^2 / 255)) next to the
       // staged image
       const uint32_t words = nrows * L.imgp / 4;
@@ -475,9 +483,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
           const uint32_t tcol = a_col0 + (s * L.rps + (r - r0)) * a_row_cols;
           const uint8_t* row = img_buf + r * L.imgp;
           if constexpr (MASKED) {
+            build_row<KS, false>(row, m, q.w, tmem_addr(tmem, lane_base, tcol));
+            if (need_y) {
 #pragma unroll
-            for (int pl = 0; pl < NPL; ++pl)
-              build_row<KS, false>(row + pl * L.plane_bytes, m, q.w, tmem_addr(tmem, lane_base, tcol + pl * KS));
+              for (int pl = 1; pl < NPL; ++pl)
+                build_row<KS, false>(row + pl * L.plane_bytes, m, q.w, tmem_addr(tmem, lane_base, tcol + pl * KS));
+            }
           } else {
             s_rs[r * kM + m] = build_row<KS, true>(row, m, q.w, tmem_addr(tmem, lane_base, tcol));
           }
@@ -521,7 +532,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t ksteps = q.kmma / 32;
       const uint4* band = reinterpret_cast<const uint4*>(smem + kBandTable);
       const bool leader = elect_one();
-      for (uint32_t st = 0; st < nst; ++st, ++g) {
+      // test hook: a wait on the drain barrier, which nothing arrives at before the end
+      if (L.stall && !__all_sync(0xffffffffu, mbar_wait(drain, 0, deadline))) ok = false;
+      for (uint32_t st = 0; ok && st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
         const bool got = mbar_wait(&full[s], (g / kStages) & 1u, deadline);
         if (!__all_sync(0xffffffffu, got)) {
@@ -548,6 +561,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
                 const uint32_t a = a_stage + (i0 + j) * a_row_cols;
 #pragma unroll
                 for (int c = 0; c < NCORR; ++c) {
+                  if (c > 0 && !need_y) break;
                   const uint32_t zo = zrow + c * zoff1;
                   const uint32_t acc = c == 0 ? 0u : 1u;  // X, or Y for both parts of I^2
 #pragma unroll
@@ -623,7 +637,8 @@ uint32_t ks_of(uint32_t w) {
 
 // Kernel-wide tile and shared-memory plan for a group sharing (ks, masked):
 // sized for the group's tallest template.
-bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl) {
+// nt_only: a tile height the plan must use (0: the tallest that fits).
+bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl, uint32_t nt_only = 0) {
   const uint32_t npl = masked ? 3 : 1, nacc = masked ? 2 : 1, nz = masked ? 3 : 1;
   pl.ks = ks;
   pl.masked = masked;
@@ -638,6 +653,7 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl)
   // after about one tile's time, which the 64-row tile keeps shorter.
   const uint32_t nts[2] = {masked ? (tall ? 96u : 64u) : 128u, 64u};
   for (uint32_t nt : nts) {
+    if (nt_only && nt != nt_only) continue;
     const uint32_t tm_left = kTmemCols - nacc * nt;
     const uint32_t rps = tm_left / (kStages * npl * ks);
     if (rps < 1) continue;
@@ -683,6 +699,7 @@ bool umma_supported(const MatchArgs& a) {
 }
 
 uint32_t umma_group_key(const MatchArgs& a) { return ks_of(a.w) * 2 + (a.mask ? 1 : 0); }
+uint32_t umma_row_width(uint32_t w) { return ks_of(w); }
 
 cudaError_t umma_prepare_kernels() {
   cudaError_t e;
@@ -694,8 +711,15 @@ cudaError_t umma_prepare_kernels() {
   return cudaSuccess;
 }
 
-bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl) {
-  return make_plan(ks, masked, hmax, /*tall=*/true, pl);
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt) {
+  if (ks < 8 || ks > (masked ? 32u : 64u) || (ks & (ks - 1))) return false;
+  return make_plan(ks, masked, hmax, /*tall=*/true, pl, nt);
+}
+
+uint32_t umma_tile_heights(bool masked, uint32_t out[2]) {
+  out[0] = masked ? 96u : 128u;
+  out[1] = 64u;
+  return 2;
 }
 
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
@@ -770,6 +794,7 @@ cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int
   L.err = err_word;
   L.tag = tag;
   L.wait_ns = pipeline_wait_ns();
+  L.stall = pipeline_stall() ? 1u : 0u;
   return launch_umma_batch(pl, L, a.stream, a.timer);
 }
 
@@ -783,11 +808,16 @@ __global__ void extremes_keys_init_kernel(unsigned long long* keys, uint32_t n) 
 }
 
 // keys -> ipb_extremes_f32 (the order key inverts exactly; indices -> (x, y))
-__global__ void extremes_keys_finish_kernel(const unsigned long long* keys, const uint32_t* widths,
+// Writes the records and re-arms the keys ({~0, 0}) for the next launch
+// of the same plan, so a replayed batch needs no separate initialisation.
+__global__ void extremes_keys_finish_kernel(unsigned long long* keys, const uint32_t* widths,
                                             ipb_extremes_f32* const* outs, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !outs[i]) return;
+  if (i >= n) return;
   const unsigned long long kmin = keys[2 * i], kmax = keys[2 * i + 1];
+  keys[2 * i] = ~0ull;
+  keys[2 * i + 1] = 0ull;
+  if (!outs[i]) return;
   auto value = [](uint32_t ok) {
     const uint32_t b = (ok & 0x80000000u) ? (ok & 0x7FFFFFFFu) : ~ok;
     return __uint_as_float(b);
@@ -810,7 +840,7 @@ cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cuda
   return cudaGetLastError();
 }
 
-cudaError_t launch_extremes_keys_finish(const unsigned long long* keys, const uint32_t* widths,
+cudaError_t launch_extremes_keys_finish(unsigned long long* keys, const uint32_t* widths,
                                         ipb_extremes_f32* const* outs, uint32_t n, cudaStream_t s) {
   if (!n) return cudaSuccess;
   extremes_keys_finish_kernel<<<(n + 255) / 256, 256, 0, s>>>(keys, widths, outs, n);

@@ -89,6 +89,11 @@ EXTREMES_DTYPE = [("max_value", "<f4"), ("min_value", "<f4"), ("max_x", "<u4"), 
                   ("min_x", "<u4"), ("min_y", "<u4")]
 
 
+class _BatchGroup(C.Structure):
+    _fields_ = [("row_width", C.c_uint32), ("tile_rows", C.c_uint32), ("masked", C.c_int),
+                ("pairs", C.c_uint32), ("tiles", C.c_uint32)]
+
+
 def _bind_batch():
     L = _lib.lib()
     if getattr(L, "_batch_bound", False):
@@ -101,6 +106,8 @@ def _bind_batch():
     L.ipb_batch_plan_launch.restype = C.c_int
     L.ipb_batch_plan_info.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.ipb_batch_plan_info.restype = C.c_int
+    L.ipb_batch_plan_groups.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(_BatchGroup), C.POINTER(C.c_uint32)]
+    L.ipb_batch_plan_groups.restype = C.c_int
     L.ipb_batch_plan_destroy.argtypes = [C.c_void_p]
     L.ipb_batch_plan_destroy.restype = C.c_int
     L._batch_bound = True
@@ -174,9 +181,17 @@ class BatchPlan:
         return self.batch.outs
 
     def info(self):
-        k, t = C.c_uint32(), C.c_uint32()
-        check(_bind_batch().ipb_batch_plan_info(self._h, C.byref(k), C.byref(t)))
-        return {"kernels": k.value, "tensor_pairs": t.value}
+        """Kernels per launch, tensor-core pairs and the tensor-core launches
+        (row width, tile rows, mask kind, pairs, tiles) in launch order."""
+        L = _bind_batch()
+        k, t, n = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(L.ipb_batch_plan_info(self._h, C.byref(k), C.byref(t)))
+        check(L.ipb_batch_plan_groups(self._h, 0, None, C.byref(n)))
+        groups = (_BatchGroup * max(n.value, 1))()
+        check(L.ipb_batch_plan_groups(self._h, n.value, groups, C.byref(n)))
+        return {"kernels": k.value, "tensor_pairs": t.value,
+                "launches": [{"row_width": g.row_width, "tile_rows": g.tile_rows, "masked": bool(g.masked),
+                              "pairs": g.pairs, "tiles": g.tiles} for g in groups[: n.value]]}
 
     def close(self):
         if self._h:

@@ -173,3 +173,55 @@ def test_batch_rejects_invalid_pair_before_any_work():
         batch.run()
     torch.cuda.synchronize()
     assert (batch.outs[0] == -1.0).all()
+
+
+def test_batch_tuner_persists_choices_and_replays_rearm_extremes(tmp_path, monkeypatch):
+    # the default group tuner times each natural group's row width and tile
+    # height, persists the choice, and a later plan reads it back; results
+    # stay bit-exact whatever the choice, and each replay re-arms the fused
+    # extremes (the second launch sees new image content)
+    import torch
+
+    from imageproc_b200 import device
+    L = _lib.lib()
+    L.ipb_batch_tuning_reset.argtypes = []
+    L.ipb_batch_tuning_reset.restype = None
+    f = tmp_path / "tuning.txt"
+    monkeypatch.setenv("IPB_TUNING_FILE", str(f))
+    monkeypatch.delenv("IPB_AUTOTUNE", raising=False)
+    L.ipb_batch_tuning_reset()
+    pairs = synthetic.uneven_pairs(n=24, seed=7, lo=128, hi=768)
+    items = [(im, tp, m, None) for im, tp, m in pairs]
+    dev_items = _to_device(items)
+    batch = device.Batch(dev_items)
+    plan = device.BatchPlan(batch)
+    info = plan.info()
+    assert info["kernels"] == len(info["launches"]) + 1  # tensor launches + the extremes finish
+    assert info["tensor_pairs"] == len(items)
+    groups = [ln.split() for ln in f.read_text().splitlines() if ln.startswith("group ")]
+    assert groups, "group decisions persisted"
+    plan.launch()
+    torch.cuda.synchronize()
+    _check(items, batch.outs, batch.extremes_host())
+    # new content in every image, same plan: extremes from this launch only
+    g = np.random.default_rng(11)
+    new_items = []
+    for (image, template, method, mask), d in zip(items, dev_items):
+        fresh = g.integers(0, 256, image.shape, dtype=np.uint8)
+        d[0].copy_(torch.from_numpy(fresh))
+        new_items.append((fresh, template, method, mask))
+    plan.launch()
+    torch.cuda.synchronize()
+    _check(new_items, batch.outs, batch.extremes_host())
+    plan.close()
+    # a persisted choice is read back: force 64-row tiles at the natural width
+    f.write_text("".join(f"group {k[1]} {k[2]} {k[3]} {k[4]} {k[5]} {k[1]} 64\n" for k in groups))
+    L.ipb_batch_tuning_reset()
+    plan2 = device.BatchPlan(batch)
+    info2 = plan2.info()
+    assert {g2["tile_rows"] for g2 in info2["launches"]} == {64}
+    plan2.launch()
+    torch.cuda.synchronize()
+    _check(new_items, batch.outs, batch.extremes_host())
+    plan2.close()
+    L.ipb_batch_tuning_reset()
