@@ -481,9 +481,9 @@ def run_learned(args, world, rank, local) -> dict:
     stream = torch.cuda.current_stream()
     net = learned.ProposalNet.trained()
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    ex_ms = le_ms = 0.0
-    agree = queries = flat = 0
-    paths = [0, 0, 0]
+    ex_ms = le_ms = l0_ms = py_ms = 0.0
+    agree = l0_agree = py_agree = queries = flat = 0
+    paths, l0_paths, py_paths = [0, 0, 0], [0, 0, 0], [0, 0, 0]
     for k, (image, templates, nflat) in enumerate(scenes):
         flat += nflat
         di = torch.from_numpy(image).to(dev)
@@ -492,6 +492,8 @@ def run_learned(args, world, rank, local) -> dict:
             for _ in range(2):
                 device.match_templates_device(di, dt, 0, scores=False, extremes=True, stream=stream)
                 net.propose_and_match(di, dt, stream=stream)
+                net.propose_and_match(di, dt, min_margin=0.0, stream=stream)
+                learned.match_proposals(di, dt, learned.pyramid_origins(di, dt), stream=stream)
         torch.cuda.synchronize()
         a, b = ev(), ev()
         a.record(stream)
@@ -505,11 +507,32 @@ def run_learned(args, world, rank, local) -> dict:
         b.record(stream)
         torch.cuda.synchronize()
         le_ms += a.elapsed_time(b)
-        for e, r in zip(exh, ans):
+        # the certificate alone (no margin gate): low-margin templates are
+        # certified where the bound allows instead of falling back
+        a, b = ev(), ev()
+        a.record(stream)
+        ans0 = net.propose_and_match(di, dt, min_margin=0.0, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        l0_ms += a.elapsed_time(b)
+        # ablation: the same verification and certification fed by coarse-pyramid
+        # proposals (torch operators for the proposals themselves)
+        a, b = ev(), ev()
+        a.record(stream)
+        pyr = learned.match_proposals(di, dt, learned.pyramid_origins(di, dt), stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        py_ms += a.elapsed_time(b)
+        for e, r, r0, pr in zip(exh, ans, ans0, pyr):
             queries += 1
             paths[r.path] += 1
-            agree += int(np.float32(e.min_value).view(np.uint32) == np.float32(r.value).view(np.uint32)
-                         and tuple(e.min_value_location) == r.location)
+            l0_paths[r0.path] += 1
+            py_paths[pr.path] += 1
+            same = lambda x: int(np.float32(e.min_value).view(np.uint32) == np.float32(x.value).view(np.uint32)  # noqa: E731
+                                 and tuple(e.min_value_location) == x.location)
+            agree += same(r)
+            l0_agree += same(r0)
+            py_agree += same(pr)
     ex_ms = max_over_ranks(ex_ms, world)
     le_ms = max_over_ranks(le_ms, world)
     ex_q = world * queries / (ex_ms / 1e3)
@@ -526,6 +549,16 @@ def run_learned(args, world, rank, local) -> dict:
         "flat_templates": flat,
         "paths": {"proposed_certified": paths[0], "fallback_low_margin": paths[1],
                   "fallback_not_certified": paths[2]},
+        "learned_certificate_only": {
+            "queries_per_s": world * queries / (max_over_ranks(l0_ms, world) / 1e3),
+            "ms_per_scene": max_over_ranks(l0_ms, world) / n_scenes, "agreement": l0_agree / max(queries, 1),
+            "proposed_certified": l0_paths[0], "fallback_not_certified": l0_paths[2],
+            "api": "ipb_propose_and_match_device, min_margin 0 (no margin gate)"},
+        "ablation_pyramid": {
+            "queries_per_s": world * queries / (max_over_ranks(py_ms, world) / 1e3),
+            "ms_per_scene": max_over_ranks(py_ms, world) / n_scenes, "agreement": py_agree / max(queries, 1),
+            "proposed_certified": py_paths[0], "fallback_not_certified": py_paths[2],
+            "api": "coarse-pyramid proposals (torch) + ipb_match_proposals_device"},
     }
 
 

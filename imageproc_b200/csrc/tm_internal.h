@@ -243,6 +243,13 @@ uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl);
 // Fills the plan fields of L and launches (L.inl / L.probs, nprobs, tiles,
 // err, tag set by the caller).
 cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t stream, KernelTimer* timer);
+// find_extremes keys (2 per template, armed by the caller) of n <= 8
+// unmasked templates of one shape against one image, in one tensor-core
+// launch without score maps.
+cudaError_t launch_umma_extremes(const uint8_t* img, uint32_t W, uint32_t H, const uint8_t* const* tpls,
+                                 uint32_t n, uint32_t w, uint32_t h, int method, int precision,
+                                 unsigned long long* keys, unsigned int* err_word, unsigned int tag,
+                                 cudaStream_t stream);
 cudaError_t launch_extremes_keys_init(unsigned long long* keys, uint32_t n, cudaStream_t s);
 // The finish kernel writes the records and re-arms the keys for the next launch.
 cudaError_t launch_extremes_keys_finish(unsigned long long* keys, const uint32_t* widths,

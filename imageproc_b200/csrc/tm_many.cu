@@ -156,8 +156,9 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
         float* o = ocol ? ocol + (size_t)half * rstride : nullptr;
         // Fast pass: each value is scored branch-free, stored at once and
         // folded into the half's smallest and largest bits (scores are never
-        // negative, so f32 bits order like the values), keeping few values
-        // live. FP64 quotients near an f32 rounding midpoint are flagged.
+        // negative, so f32 bits order like the values). FP64 quotients near
+        // an f32 rounding midpoint are flagged.
+        uint32_t b[16];
         uint32_t mn = 0xFFFFFFFFu, mx = 0u;
         bool undecided = false;
         {
@@ -176,25 +177,21 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
             constexpr bool kFull = decltype(full_tag)::value;
 #pragma unroll
             for (int k = 0; k < 16; k += 2) {
-              uint32_t b0, b1;
               if constexpr (kNormW) {
                 const double2 r2 = *reinterpret_cast<const double2*>(s_ryw + half + k);
-                b0 = norm_bits_fp64_fast(score_of(v[k], Y[k]), __dmul_rn(r2.x, rT), undecided);
-                b1 = norm_bits_fp64_fast(score_of(v[k + 1], Y[k + 1]), __dmul_rn(r2.y, rT), undecided);
+                b[k] = norm_bits_fp64_fast(score_of(v[k], Y[k]), __dmul_rn(r2.x, rT), undecided);
+                b[k + 1] = norm_bits_fp64_fast(score_of(v[k + 1], Y[k + 1]), __dmul_rn(r2.y, rT), undecided);
               } else {
-                b0 = __float_as_uint(finish_score32(kMethod, kPrec, v[k], Y[k], tss));
-                b1 = __float_as_uint(finish_score32(kMethod, kPrec, v[k + 1], Y[k + 1], tss));
+                b[k] = __float_as_uint(finish_score32(kMethod, kPrec, v[k], Y[k], tss));
+                b[k + 1] = __float_as_uint(finish_score32(kMethod, kPrec, v[k + 1], Y[k + 1], tss));
               }
-              if (kFull || k < nv) {
-                if (o) o[(size_t)k * rstride] = __uint_as_float(b0);
-                mn = min(mn, b0);
-                mx = max(mx, b0);
-              }
-              if (kFull || k + 1 < nv) {
-                if (o) o[(size_t)(k + 1) * rstride] = __uint_as_float(b1);
-                mn = min(mn, b1);
-                mx = max(mx, b1);
-              }
+#pragma unroll
+              for (int u = 0; u < 2; ++u)
+                if (kFull || k + u < nv) {
+                  if (o) o[(size_t)(k + u) * rstride] = __uint_as_float(b[k + u]);
+                  mn = min(mn, b[k + u]);
+                  mx = max(mx, b[k + u]);
+                }
             }
           };
           if (nv == 16)
@@ -202,52 +199,56 @@ __device__ __forceinline__ bool epilogue(EpiCtx& c) {
           else
             pass(std::false_type{});
         }
-        // Second pass, rare and warp-uniform: a half with a flagged or
-        // zero-norm quotient (re-stored through the general quotient), or
-        // whose extremes could beat this lane's running keys (the keys with
-        // the half's first index bound what the half can contribute). The
-        // sums are reloaded and the first occurrence of each extreme found.
-        const uint32_t idx0 = (c.y0 + mb + half) * p.Wo + x;
-        const bool want_ext =
-            kExt && t_ok &&
-            ((((unsigned long long)(mn | 0x80000000u) << 32) | idx0) < c.kmin ||
-             (((unsigned long long)(mx | 0x80000000u) << 32) | (0xFFFFFFFFu - idx0)) > c.kmax);
-        const bool fix = general || undecided;
-        if (__any_sync(0xffffffffu, fix || want_ext)) {
+        // Rare and warp-uniform: a half with a flagged or zero-norm quotient
+        // reloads its sums, re-scores the flagged values through the general
+        // quotient, stores them again and recomputes the half's extremes.
+        if (__any_sync(0xffffffffu, general || undecided)) {
           uint32_t v[16];
           tmem_ld16(taddr, v);
           tmem_wait_ld();
-          uint32_t bmn = 0xFFFFFFFFu, jmn = 0, bmx = 0u, jmx = 0;
+          if constexpr (kNormW) {
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            if (k >= nv) break;
-            const uint32_t yk = ycol[half + k];
-            const uint32_t s = score_of(v[k], yk);
-            uint32_t bk;
-            if constexpr (kNormW) {
+            for (int k = 0; k < 16; ++k) {
+              if (k >= nv) break;
+              const uint32_t yk = ycol[half + k];
+              const uint32_t sk = score_of(v[k], yk);
               const double w = __dmul_rn(s_ryw[half + k], rT);
               bool u = general;
-              bk = general ? 0u : norm_bits_fp64_fast(s, w, u);
+              if (!general) norm_bits_fp64_fast(sk, w, u);
               if (u) {
-                bk = __float_as_uint(norm_quotient_fp64_w(s, w, yk, tss));
-                if (o) o[(size_t)k * rstride] = __uint_as_float(bk);
+                b[k] = __float_as_uint(norm_quotient_fp64_w(sk, w, yk, tss));
+                if (o) o[(size_t)k * rstride] = __uint_as_float(b[k]);
               }
-            } else {
-              bk = __float_as_uint(finish_score32(kMethod, kPrec, v[k], yk, tss));
-            }
-            if (bk < bmn) {
-              bmn = bk;
-              jmn = k;
-            }
-            if (bk > bmx) {
-              bmx = bk;
-              jmx = k;
             }
           }
-          if (kExt && t_ok) {
-            c.kmin = min(c.kmin, ((unsigned long long)(bmn | 0x80000000u) << 32) | (idx0 + jmn * p.Wo));
-            c.kmax = max(c.kmax,
-                         ((unsigned long long)(bmx | 0x80000000u) << 32) | (0xFFFFFFFFu - (idx0 + jmx * p.Wo)));
+          mn = 0xFFFFFFFFu;
+          mx = 0u;
+#pragma unroll
+          for (int k = 0; k < 16; ++k)
+            if (k < nv) {
+              mn = min(mn, b[k]);
+              mx = max(mx, b[k]);
+            }
+        }
+        if constexpr (kExt) {
+          // the half's extremes reach this lane's running keys only when the
+          // key with the half's first index does (the 16 positions are rows of
+          // one column: the lowest k is the lowest index); then the first
+          // occurrence is found in this lane alone
+          const uint32_t idx0 = (c.y0 + mb + half) * p.Wo + x;
+          if (t_ok && ((((unsigned long long)(mn | 0x80000000u) << 32) | idx0) < c.kmin)) {
+            uint32_t j = 0;
+#pragma unroll
+            for (int k = 15; k >= 0; --k)
+              if (b[k] == mn) j = k;
+            c.kmin = min(c.kmin, ((unsigned long long)(mn | 0x80000000u) << 32) | (idx0 + j * p.Wo));
+          }
+          if (t_ok && ((((unsigned long long)(mx | 0x80000000u) << 32) | (0xFFFFFFFFu - idx0)) > c.kmax)) {
+            uint32_t j = 0;
+#pragma unroll
+            for (int k = 15; k >= 0; --k)
+              if (b[k] == mx) j = k;
+            c.kmax = max(c.kmax, ((unsigned long long)(mx | 0x80000000u) << 32) | (0xFFFFFFFFu - (idx0 + j * p.Wo)));
           }
         }
       }

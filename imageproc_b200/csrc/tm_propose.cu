@@ -22,9 +22,12 @@
 //      a lower bound for the whole block from two tables built once per
 //      image. Blocks whose bound exceeds the verified minimum cannot hold the
 //      answer; the others must lie inside a verified window, or are verified
-//      too (up to a budget) -- otherwise the template falls back;
+//      too, one warp per 4 x 4 block (verify_blocks_kernel, up to 16384
+//      blocks per template) -- otherwise the template falls back;
 //   5. templates whose margin is below the threshold, or that could not be
-//      certified, are answered by the exhaustive many-templates kernel.
+//      certified, are answered exhaustively: up to 8 of them by one
+//      single-template tensor-core launch (extremes only), more by the
+//      many-templates kernel.
 // A certified answer equals find_extremes' minimum of the exhaustive map
 // exactly: every position outside the verified set has a larger score.
 #include <algorithm>
@@ -48,7 +51,9 @@ constexpr int kCell = 8;          // heatmap cell: 8 x 8 downsampled positions
 constexpr int kMaxTopK = 16;
 constexpr int kWin = 32;          // verification window: 32 x 32 positions
 constexpr int kBlk = 12;          // certification block: 12 x 12 positions
-constexpr int kMaxExtra = 512;    // most extra 4 x 4 blocks a template may verify
+constexpr int kMaxExtra = 16384;  // most extra 4 x 4 blocks a template may verify
+constexpr int kVerifySlices = 32;  // blocks of threads per template verifying extra blocks
+constexpr uint32_t kFallbackPerTemplate = 8;  // fallbacks up to this many use the single-template kernel
 constexpr int kPatch = kWin + kTpl - 1;        // 79 image rows / columns per window
 constexpr int kPatchPitch = 96;                // 16-byte multiple >= kPatch + 4
 
@@ -539,7 +544,7 @@ __global__ void __launch_bounds__(256) certify_kernel(const uint8_t* __restrict_
                                                       const uint32_t* __restrict__ span16, uint32_t Mx, uint32_t My,
                                                       uint32_t Wo, uint32_t Ho, const Rect* __restrict__ wins,
                                                       const uint32_t* __restrict__ nwin, uint32_t max_rects,
-                                                      Rect* __restrict__ extra, uint32_t* __restrict__ n_extra) {
+                                                      uint32_t* __restrict__ extra, uint32_t* __restrict__ n_extra) {
   __shared__ uint32_t s_st[16];
   __shared__ Rect s_win[kMaxTopK];
   const uint32_t t = blockIdx.x;
@@ -592,10 +597,119 @@ __global__ void __launch_bounds__(256) certify_kernel(const uint8_t* __restrict_
         }
         if (covered) continue;
         const uint32_t slot = atomicAdd(n_extra + t, 1u);
-        if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = Rect{x0, y0, x1 - x0, y1 - y0};
+        if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = py * Pmx + px;
       }
     }
   }
+}
+
+// Exact minimum over the extra blocks of 4 x 4 positions (packed micro-block
+// indices py * Pmx + px from certify_kernel), every block of every template
+// whose list fits: grid (slices, template), one warp per block, lanes = 16
+// positions x 2 halves of the template's rows. Each lane sums X = sum I*T and
+// Y = sum I^2 over its 24 rows with dp4a on aligned image words (read through
+// the cache; W * H is a multiple of 4, so no word crosses the image's end)
+// shifted by byte_perm, the halves meet through one shuffle, and SSE =
+// Y - 2X + TSS rounds once to f32 as in verify_kernel. The first minimum goes
+// to best[t].
+__global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __restrict__ img, uint32_t W,
+                                                            const uint8_t* __restrict__ tpl,
+                                                            const uint32_t* __restrict__ extra,
+                                                            const uint32_t* __restrict__ n_extra, uint32_t Pmx,
+                                                            uint32_t Wo, uint32_t Ho,
+                                                            unsigned long long* __restrict__ best) {
+  __shared__ uint32_t s_tpl[kTpl][kTpl / 4 + 1];  // padded: the two row halves fall in different banks
+  __shared__ unsigned long long s_tss[8];
+  __shared__ unsigned long long s_best[8];
+  const uint32_t t = blockIdx.y;
+  const uint32_t n = n_extra[t];
+  if (n == 0 || n > (uint32_t)kMaxExtra) return;  // nothing listed, or the template falls back
+  const uint32_t* tw = reinterpret_cast<const uint32_t*>(tpl + (size_t)t * kTpl * kTpl);
+  unsigned long long tss = 0ull;
+  for (uint32_t i = threadIdx.x; i < (uint32_t)(kTpl * kTpl / 4); i += blockDim.x) {
+    const uint32_t v = tw[i];
+    s_tpl[i / (kTpl / 4)][i % (kTpl / 4)] = v;
+    tss += __dp4a(v, v, 0u);
+  }
+  for (int d = 16; d; d >>= 1) tss += __shfl_xor_sync(0xffffffffu, tss, d);
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) s_tss[warp] = tss;
+  __syncthreads();
+  tss = 0ull;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tss += s_tss[k];
+  const uint32_t pos = lane & 15u, half = lane >> 4;
+  const uint32_t ox = pos & 3u, oy = pos >> 2;
+  unsigned long long mykey = ~0ull;
+  const uint32_t* const img32 = reinterpret_cast<const uint32_t*>(img);
+  for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + warp; i < n; i += gridDim.x * (blockDim.x >> 5)) {
+    const uint32_t mb = extra[(size_t)t * kMaxExtra + i];
+    const uint32_t x = 4 * (mb % Pmx) + ox, y = 4 * (mb / Pmx) + oy;
+    const bool valid = x < Wo && y < Ho;
+    const uint32_t xs = valid ? x : 0u, ys = valid ? y : 0u;  // in-bounds reads for the block's edge lanes
+    uint32_t X = 0u, Y = 0u;
+#pragma unroll 2
+    for (uint32_t dy = half * (kTpl / 2); dy < (half + 1) * (kTpl / 2); ++dy) {
+      const size_t a = (size_t)(ys + dy) * W + xs;
+      const uint32_t* row = img32 + (a >> 2);
+      const uint32_t sel = 0x3210u + (uint32_t)(a & 3u) * 0x1111u;
+      uint32_t cur = __ldg(row);
+#pragma unroll
+      for (int k = 0; k < kTpl / 4; ++k) {
+        // the word after the window's last byte is read only when the window is unaligned
+        const uint32_t nxt = (k + 1 < kTpl / 4 || (a & 3u)) ? __ldg(row + k + 1) : 0u;
+        const uint32_t iw = __byte_perm(cur, nxt, sel);
+        X = __dp4a(iw, s_tpl[dy][k], X);
+        Y = __dp4a(iw, iw, Y);
+        cur = nxt;
+      }
+    }
+    X += __shfl_xor_sync(0xffffffffu, X, 16);
+    Y += __shfl_xor_sync(0xffffffffu, Y, 16);
+    if (valid && half == 0) {
+      const unsigned long long sse = (unsigned long long)Y + tss - 2ull * X;
+      const float score = (float)sse;  // round to nearest
+      const unsigned long long key = ((unsigned long long)okey(score) << 32) | (y * Wo + x);
+      mykey = key < mykey ? key : mykey;
+    }
+  }
+  for (int d = 16; d; d >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, mykey, d);
+    mykey = o < mykey ? o : mykey;
+  }
+  if (lane == 0) s_best[warp] = mykey;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long b = s_best[0];
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = s_best[k] < b ? s_best[k] : b;
+    if (b != ~0ull) atomicMin(best + t, b);
+  }
+}
+
+// Windows of caller-given proposals: template origins (y * Wo + x, k per
+// template), each the centre of a 32 x 32 window moved inside the map; the
+// proposals carry no confidence (margin +inf: never below the threshold).
+__global__ void origin_windows_kernel(const uint32_t* __restrict__ origins, uint32_t T, uint32_t k, uint32_t Wo,
+                                      uint32_t Ho, TopK* __restrict__ tk, Rect* __restrict__ rects,
+                                      uint32_t* __restrict__ counts, uint32_t max_rects,
+                                      unsigned long long* __restrict__ best, uint32_t* __restrict__ n_extra) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const uint32_t ww = Wo < (uint32_t)kWin ? Wo : kWin, wh = Ho < (uint32_t)kWin ? Ho : kWin;
+  for (uint32_t i = 0; i < k; ++i) {
+    const uint32_t o = origins[(size_t)t * k + i];
+    const uint32_t ox = o % Wo, oy = min(o / Wo, Ho - 1u);
+    int cx = (int)ox - kWin / 2, cy = (int)oy - kWin / 2;
+    cx = cx < 0 ? 0 : (cx > (int)(Wo - ww) ? (int)(Wo - ww) : cx);
+    cy = cy < 0 ? 0 : (cy > (int)(Ho - wh) ? (int)(Ho - wh) : cy);
+    rects[(size_t)t * max_rects + i] = Rect{(uint32_t)cx, (uint32_t)cy, ww, wh};
+    tk[t].pos[i] = o;
+    tk[t].logit[i] = 0.0f;
+  }
+  tk[t].margin = __int_as_float(0x7f800000);  // +inf
+  tk[t].count = k;
+  counts[t] = k;
+  best[t] = ~0ull;
+  n_extra[t] = 0;
 }
 
 }  // namespace
@@ -663,7 +777,7 @@ struct Carve {
   TopK* tk;
   Rect* wins;
   uint32_t* nwin;
-  Rect* extra;
+  uint32_t* extra;  // per template: kMaxExtra packed micro-block indices
   uint32_t* n_extra;
   unsigned long long* best;
   uint32_t* micro;
@@ -698,7 +812,7 @@ Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
   c.tk = reinterpret_cast<TopK*>(take((size_t)T * sizeof(TopK)));
   c.wins = reinterpret_cast<Rect*>(take((size_t)T * k * sizeof(Rect)));
   c.nwin = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
-  c.extra = reinterpret_cast<Rect*>(take((size_t)T * kMaxExtra * sizeof(Rect)));
+  c.extra = reinterpret_cast<uint32_t*>(take((size_t)T * kMaxExtra * sizeof(uint32_t)));
   c.n_extra = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
   c.best = reinterpret_cast<unsigned long long*>(take((size_t)T * 8));
   const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
@@ -728,34 +842,12 @@ ProposeScratch& scratch_for_thread() {
   return s;
 }
 
-}  // namespace
 
-IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, const uint8_t* d_image,
-                                                uint32_t image_width, uint32_t image_height,
-                                                const uint8_t* d_templates, uint32_t template_width,
-                                                uint32_t template_height, uint32_t n_templates, int method,
-                                                const ipb_propose_options* options, ipb_proposal_result* results,
-                                                void* stream) {
-  const uint32_t W = image_width, H = image_height, T = n_templates;
-  if (!net || !d_image || !d_templates || !results) return pfail(IPB_ERR_INVALID_ARGUMENT, "null argument");
-  if (template_width != (uint32_t)kTpl || template_height != (uint32_t)kTpl)
-    return pfail(IPB_ERR_INVALID_ARGUMENT, "the proposal network takes 48 x 48 templates");
-  if (method != IPB_SUM_OF_SQUARED_ERRORS)
-    return pfail(IPB_ERR_INVALID_ARGUMENT,
-                 "learned proposals answer SumOfSquaredErrors queries (their certificate bounds that score)");
-  if (W % 32 || H % 32 || W < 64 || H < 64)
-    return pfail(IPB_ERR_INVALID_ARGUMENT, "learned proposals take images whose sides are multiples of 32 (>= 64)");
-  if (T == 0) return IPB_OK;
-  ipb_propose_options opt{16u, 0.1f, 1};
-  if (options) opt = *options;
-  if (opt.top_k == 0 || opt.top_k > (uint32_t)kMaxTopK)
-    return pfail(IPB_ERR_INVALID_ARGUMENT, "top_k must be 1..16");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  ProposeScratch& ps = scratch_for_thread();
+// Scratch of this thread for a query of W x H and T templates (grown, never shrunk).
+ipb_status acquire_scratch(ProposeScratch& ps, size_t bytes) {
   int dev = 0;
   P_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
-  const Carve need = carve(nullptr, W, H, T, opt.top_k);
-  if (ps.device != dev || ps.bytes < need.bytes) {
+  if (ps.device != dev || ps.bytes < bytes) {
     if (ps.p) {
       P_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
       cudaFree(ps.p);
@@ -767,46 +859,39 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
       ps.err = nullptr;
     }
     ps.device = dev;
-    P_CUDA(cudaMalloc(&ps.p, need.bytes), "cudaMalloc (proposal scratch)");
-    ps.bytes = need.bytes;
+    P_CUDA(cudaMalloc(&ps.p, bytes), "cudaMalloc (proposal scratch)");
+    ps.bytes = bytes;
     if (!ps.err) {
       P_CUDA(cudaMalloc(&ps.err, sizeof(unsigned int)), "cudaMalloc");
       P_CUDA(cudaMemset(ps.err, 0, sizeof(unsigned int)), "cudaMemset");
     }
   }
-  const Carve c = carve(static_cast<uint8_t*>(ps.p), W, H, T, opt.top_k);
-  const PackedWeights& pw = net_weights(net);
-  const uint32_t Hs = H / 4, Ws = W / 4, Wo = W - kTpl + 1, Ho = H - kTpl + 1;
-  const uint32_t Cx = Ws / kCell, Cy = Hs / kCell;
-  const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
+  return IPB_OK;
+}
 
-  // 1. trunk of the image and of the templates, embedding, heatmap cells
-  // one tag for every tensor-core launch of this call: a bounded wait that runs
-  // out in any of them leaves a value >= it in the error word
-  const unsigned int call_tag = ++ps.tag;
-  const int conv_kernel = use_mma_kernels() ? 1 : 0;
-  P_CUDA(launch_trunk(d_image, 1, H, W, pw, nullptr, c.a, c.b, c.F, s, conv_kernel, ps.err, call_tag),
-         "image trunk");
-  P_CUDA(launch_trunk(d_templates, T, kTpl, kTpl, pw, nullptr, c.ta, c.tb, c.Ft, s, conv_kernel, ps.err, call_tag),
-         "template trunk");
-  P_CUDA(launch_embed(c.Ft, T, c.G, s), "embedding");
-  pack_embedding_kernel<<<(T * kEmb + 255) / 256, 256, 0, s>>>(c.G, T, c.gb);
-  count_launch(kKernelPropose);
-  if (use_mma_kernels()) {
-    const dim3 hg((Ws + kHW - 1) / kHW, Hs / kCell, (T + 31) / 32);
-    head_cells_kernel<<<hg, 256, 0, s>>>(c.F, Hs, Ws, c.gb, T, c.cells);
-    count_launch(kKernelPropose);
-    P_CUDA(cudaGetLastError(), "heatmap");
-  } else {
-    P_CUDA(launch_head_tc(c.F, Hs, Ws, c.gb, T, c.cells, ps.err, call_tag, s), "heatmap");
-  }
-  // 2. top-k and margins
-  topk_kernel<<<T, 512, 0, s>>>(c.cells, Cy, Cx, Ws, opt.top_k, c.tk);
-  count_launch(kKernelPropose);
-  // 3. windows and their exact scores
-  windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(c.tk, T, Ws, Wo, Ho, c.wins, c.nwin, opt.top_k, c.best,
-                                                 c.n_extra);
-  count_launch(kKernelPropose);
+// Checks shared by the query entry points.
+ipb_status check_query(const uint8_t* d_image, uint32_t W, uint32_t H, const uint8_t* d_templates,
+                       uint32_t template_width, uint32_t template_height, int method, const char* who) {
+  if (!d_image || !d_templates) return pfail(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (template_width != (uint32_t)kTpl || template_height != (uint32_t)kTpl)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, std::string(who) + " take 48 x 48 templates");
+  if (method != IPB_SUM_OF_SQUARED_ERRORS)
+    return pfail(IPB_ERR_INVALID_ARGUMENT,
+                 std::string(who) + " answer SumOfSquaredErrors queries (their certificate bounds that score)");
+  if (W % 32 || H % 32 || W < 64 || H < 64)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, std::string(who) + " take images whose sides are multiples of 32 (>= 64)");
+  if ((reinterpret_cast<uintptr_t>(d_image) | reinterpret_cast<uintptr_t>(d_templates)) & 15u)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, std::string(who) + " take 16-byte aligned image and template buffers");
+  return IPB_OK;
+}
+
+// Steps 3 (after the windows are set) to 5: exact scores of the windows,
+// certification, verdicts and the exhaustive fallback, into results.
+ipb_status finish_queries(ProposeScratch& ps, const Carve& c, unsigned int call_tag, const uint8_t* d_image,
+                          uint32_t W, uint32_t H, const uint8_t* d_templates, uint32_t T,
+                          const ipb_propose_options& opt, ipb_proposal_result* results, cudaStream_t s) {
+  const uint32_t Wo = W - kTpl + 1, Ho = H - kTpl + 1;
+  const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
   verify_kernel<<<dim3(opt.top_k, T), 256, 0, s>>>(d_image, W, H, d_templates, c.wins, c.nwin, opt.top_k, c.best);
   count_launch(kKernelPropose);
   P_CUDA(cudaGetLastError(), "verification");
@@ -822,8 +907,8 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
                                                         c.span16, Mx, My, Wo, Ho, c.wins, c.nwin, opt.top_k,
                                                         c.extra, c.n_extra);
     count_launch(kKernelPropose);
-    verify_kernel<<<dim3(kMaxExtra, T), 256, 0, s>>>(d_image, W, H, d_templates, c.extra, c.n_extra, kMaxExtra,
-                                                     c.best);
+    verify_blocks_kernel<<<dim3(kVerifySlices, T), 256, 0, s>>>(d_image, W, d_templates, c.extra, c.n_extra,
+                                                                   (Wo + 3) / 4, Wo, Ho, c.best);
     count_launch(kKernelPropose);
     P_CUDA(cudaGetLastError(), "certification");
   }
@@ -852,15 +937,26 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
   }
   std::vector<ipb_extremes_f32> fb_ext(fb.size());
   if (!fb.empty()) {
-    for (size_t i = 0; i < fb.size(); ++i)
-      P_CUDA(cudaMemcpyAsync(c.fb_tpl + i * kTpl * kTpl, d_templates + (size_t)fb[i] * kTpl * kTpl, kTpl * kTpl,
-                             cudaMemcpyDeviceToDevice, s),
-             "gather fallback templates");
     const uint32_t nf = (uint32_t)fb.size();
     P_CUDA(launch_many_keys_init(c.fb_keys, nf, s), "extremes init");
-    P_CUDA(launch_many(d_image, W, H, c.fb_tpl, kTpl, kTpl, nf, IPB_SUM_OF_SQUARED_ERRORS,
-                       IPB_PRECISION_EXACT_FP64, nullptr, c.fb_keys, ps.err, call_tag, s, nullptr),
-           "exhaustive fallback");
+    if (nf <= kFallbackPerTemplate) {
+      // a few templates: one single-template tensor-core launch over them
+      // (its cost grows with the templates; the many-templates kernel's
+      // hardly does below one block of templates)
+      const uint8_t* tp[kFallbackPerTemplate];
+      for (uint32_t i = 0; i < nf; ++i) tp[i] = d_templates + (size_t)fb[i] * kTpl * kTpl;
+      P_CUDA(launch_umma_extremes(d_image, W, H, tp, nf, kTpl, kTpl, IPB_SUM_OF_SQUARED_ERRORS,
+                                  IPB_PRECISION_EXACT_FP64, c.fb_keys, ps.err, call_tag, s),
+             "exhaustive fallback");
+    } else {
+      for (size_t i = 0; i < fb.size(); ++i)
+        P_CUDA(cudaMemcpyAsync(c.fb_tpl + i * kTpl * kTpl, d_templates + (size_t)fb[i] * kTpl * kTpl, kTpl * kTpl,
+                               cudaMemcpyDeviceToDevice, s),
+               "gather fallback templates");
+      P_CUDA(launch_many(d_image, W, H, c.fb_tpl, kTpl, kTpl, nf, IPB_SUM_OF_SQUARED_ERRORS,
+                         IPB_PRECISION_EXACT_FP64, nullptr, c.fb_keys, ps.err, call_tag, s, nullptr),
+             "exhaustive fallback");
+    }
     P_CUDA(launch_many_keys_finish(c.fb_keys, Wo, c.fb_ext, nf, s), "extremes finish");
     P_CUDA(cudaMemcpyAsync(fb_ext.data(), c.fb_ext, sizeof(ipb_extremes_f32) * nf, cudaMemcpyDeviceToHost, s),
            "copy fallback results");
@@ -889,4 +985,93 @@ IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, con
     }
   }
   return IPB_OK;
+}
+
+}  // namespace
+
+IPB_API ipb_status ipb_match_proposals_device(const uint8_t* d_image, uint32_t image_width, uint32_t image_height,
+                                              const uint8_t* d_templates, uint32_t template_width,
+                                              uint32_t template_height, uint32_t n_templates, int method,
+                                              const uint32_t* d_origins, uint32_t k,
+                                              const ipb_propose_options* options, ipb_proposal_result* results,
+                                              void* stream) {
+  const uint32_t W = image_width, H = image_height, T = n_templates;
+  if (!results || (T && !d_origins)) return pfail(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  ipb_status st = check_query(d_image, W, H, d_templates, template_width, template_height, method,
+                              "proposal verification and certification");
+  if (st != IPB_OK) return st;
+  if (k == 0 || k > (uint32_t)kMaxTopK) return pfail(IPB_ERR_INVALID_ARGUMENT, "k must be 1..16");
+  if (T == 0) return IPB_OK;
+  ipb_propose_options opt{k, 0.1f, 1};
+  if (options) opt = *options;
+  opt.top_k = k;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ProposeScratch& ps = scratch_for_thread();
+  if ((st = acquire_scratch(ps, carve(nullptr, W, H, T, k).bytes)) != IPB_OK) return st;
+  const Carve c = carve(static_cast<uint8_t*>(ps.p), W, H, T, k);
+  const unsigned int call_tag = ++ps.tag;
+  origin_windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(d_origins, T, k, W - kTpl + 1, H - kTpl + 1, c.tk, c.wins,
+                                                        c.nwin, k, c.best, c.n_extra);
+  count_launch(kKernelPropose);
+  P_CUDA(cudaGetLastError(), "proposal windows");
+  return finish_queries(ps, c, call_tag, d_image, W, H, d_templates, T, opt, results, s);
+}
+
+IPB_API ipb_status ipb_propose_and_match_device(const ipb_proposal_net* net, const uint8_t* d_image,
+                                                uint32_t image_width, uint32_t image_height,
+                                                const uint8_t* d_templates, uint32_t template_width,
+                                                uint32_t template_height, uint32_t n_templates, int method,
+                                                const ipb_propose_options* options, ipb_proposal_result* results,
+                                                void* stream) {
+  const uint32_t W = image_width, H = image_height, T = n_templates;
+  if (!net || !results) return pfail(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  {
+    const ipb_status st = check_query(d_image, W, H, d_templates, template_width, template_height, method,
+                                      "learned proposals");
+    if (st != IPB_OK) return st;
+  }
+  if (T == 0) return IPB_OK;
+  ipb_propose_options opt{16u, 0.1f, 1};
+  if (options) opt = *options;
+  if (opt.top_k == 0 || opt.top_k > (uint32_t)kMaxTopK)
+    return pfail(IPB_ERR_INVALID_ARGUMENT, "top_k must be 1..16");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ProposeScratch& ps = scratch_for_thread();
+  {
+    const ipb_status st = acquire_scratch(ps, carve(nullptr, W, H, T, opt.top_k).bytes);
+    if (st != IPB_OK) return st;
+  }
+  const Carve c = carve(static_cast<uint8_t*>(ps.p), W, H, T, opt.top_k);
+  const PackedWeights& pw = net_weights(net);
+  const uint32_t Hs = H / 4, Ws = W / 4, Wo = W - kTpl + 1, Ho = H - kTpl + 1;
+  const uint32_t Cx = Ws / kCell, Cy = Hs / kCell;
+
+  // 1. trunk of the image and of the templates, embedding, heatmap cells
+  // one tag for every tensor-core launch of this call: a bounded wait that runs
+  // out in any of them leaves a value >= it in the error word
+  const unsigned int call_tag = ++ps.tag;
+  const int conv_kernel = use_mma_kernels() ? 1 : 0;
+  P_CUDA(launch_trunk(d_image, 1, H, W, pw, nullptr, c.a, c.b, c.F, s, conv_kernel, ps.err, call_tag),
+         "image trunk");
+  P_CUDA(launch_trunk(d_templates, T, kTpl, kTpl, pw, nullptr, c.ta, c.tb, c.Ft, s, conv_kernel, ps.err, call_tag),
+         "template trunk");
+  P_CUDA(launch_embed(c.Ft, T, c.G, s), "embedding");
+  pack_embedding_kernel<<<(T * kEmb + 255) / 256, 256, 0, s>>>(c.G, T, c.gb);
+  count_launch(kKernelPropose);
+  if (use_mma_kernels()) {
+    const dim3 hg((Ws + kHW - 1) / kHW, Hs / kCell, (T + 31) / 32);
+    head_cells_kernel<<<hg, 256, 0, s>>>(c.F, Hs, Ws, c.gb, T, c.cells);
+    count_launch(kKernelPropose);
+    P_CUDA(cudaGetLastError(), "heatmap");
+  } else {
+    P_CUDA(launch_head_tc(c.F, Hs, Ws, c.gb, T, c.cells, ps.err, call_tag, s), "heatmap");
+  }
+  // 2. top-k and margins
+  topk_kernel<<<T, 512, 0, s>>>(c.cells, Cy, Cx, Ws, opt.top_k, c.tk);
+  count_launch(kKernelPropose);
+  // 3. windows and their exact scores
+  windows_kernel<<<(T + 127) / 128, 128, 0, s>>>(c.tk, T, Ws, Wo, Ho, c.wins, c.nwin, opt.top_k, c.best,
+                                                 c.n_extra);
+  count_launch(kKernelPropose);
+  return finish_queries(ps, c, call_tag, d_image, W, H, d_templates, T, opt, results, s);
 }

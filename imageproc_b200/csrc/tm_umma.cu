@@ -220,18 +220,35 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
       }
     }
     tmem_wait_ld();
+    // scores are never negative, so their f32 bits order like the values;
+    // the lane's 16 positions are rows of one column in index order, so the
+    // strict comparisons keep each extreme's first occurrence in the batch
+    const uint32_t y_first = e.y0 + n0;
+    const int nv = e.x < q.Wo ? (y_first < q.Ho ? (int)min(16u, q.Ho - y_first) : 0) : 0;
+    uint32_t mn = 0xFFFFFFFFu, jmn = 0, mx = 0u, jmx = 0;
+    float* orow = q.out ? q.out + (size_t)y_first * q.Wo + e.x : nullptr;  // null: extremes only
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-      const uint32_t y = e.y0 + n0 + k;
-      if (e.x < q.Wo && y < q.Ho) {
-        const float f = finish_score32(kMethod, kPrec, vx[k], yv[k], e.tss);
-        const uint32_t lin = y * q.Wo + e.x;
-        q.out[(size_t)lin] = f;
+      const uint32_t bk = __float_as_uint(finish_score32(kMethod, kPrec, vx[k], yv[k], e.tss));
+      if (k < nv) {
+        if (orow) orow[(size_t)k * q.Wo] = __uint_as_float(bk);
         if constexpr (kExt) {
-          const unsigned long long key = (unsigned long long)order_key(f) << 32;
-          kmin = min(kmin, key | lin);
-          kmax = max(kmax, key | (0xFFFFFFFFu - lin));
+          if (bk < mn) {
+            mn = bk;
+            jmn = k;
+          }
+          if (bk > mx) {
+            mx = bk;
+            jmx = k;
+          }
         }
+      }
+    }
+    if constexpr (kExt) {
+      if (nv > 0) {
+        const uint32_t lin0 = y_first * q.Wo + e.x;
+        kmin = min(kmin, ((unsigned long long)(mn | 0x80000000u) << 32) | (lin0 + jmn * q.Wo));
+        kmax = max(kmax, ((unsigned long long)(mx | 0x80000000u) << 32) | (0xFFFFFFFFu - (lin0 + jmx * q.Wo)));
       }
     }
   }
@@ -782,6 +799,32 @@ cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t st
   count_launch(kKernelUmma);
   timer_end(timer, stream);
   return e;
+}
+
+cudaError_t launch_umma_extremes(const uint8_t* img, uint32_t W, uint32_t H, const uint8_t* const* tpls,
+                                 uint32_t n, uint32_t w, uint32_t h, int method, int precision,
+                                 unsigned long long* keys, unsigned int* err_word, unsigned int tag,
+                                 cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if (n > kInlineProblems || !umma_shape_ok(w, h, false)) return cudaErrorNotSupported;
+  UmmaPlan pl;
+  if (!make_plan(ks_of(w), false, h, /*tall=*/true, pl)) return cudaErrorNotSupported;
+  cudaError_t e = umma_prepare_kernels();
+  if (e != cudaSuccess) return e;
+  UmmaLaunch L{};
+  uint32_t tiles = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const MatchArgs a{img, W, H, tpls[i], w, h, nullptr, false, method, precision, nullptr, stream};
+    L.inl[i] = umma_problem(a, pl, tiles, keys + 2 * i);
+    tiles += umma_problem_tiles(L.inl[i], pl);
+  }
+  L.nprobs = n;
+  L.tiles = tiles;
+  L.err = err_word;
+  L.tag = tag;
+  L.wait_ns = pipeline_wait_ns();
+  L.stall = pipeline_stall() ? 1u : 0u;
+  return launch_umma_batch(pl, L, stream, nullptr);
 }
 
 cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag) {

@@ -66,9 +66,11 @@ def _bind():
     L.ipb_propose_and_match_device.argtypes = [vp, vp, u32, u32, vp, u32, u32, u32, C.c_int,
                                                C.POINTER(ProposeOptions), C.POINTER(ProposalResult), vp]
     L.ipb_proposal_net_features.argtypes = [vp, vp, u32, u32, C.c_int, vp, vp]
+    L.ipb_match_proposals_device.argtypes = [vp, u32, u32, vp, u32, u32, u32, C.c_int, vp, u32,
+                                             C.POINTER(ProposeOptions), C.POINTER(ProposalResult), vp]
     for f in ("ipb_proposal_net_create", "ipb_proposal_net_destroy", "ipb_proposal_net_get_params",
               "ipb_proposal_net_gradients", "ipb_proposal_net_train_step", "ipb_propose_and_match_device",
-              "ipb_proposal_net_features"):
+              "ipb_proposal_net_features", "ipb_match_proposals_device"):
         getattr(L, f).restype = C.c_int
     L._learned_bound = True
     return L
@@ -192,6 +194,55 @@ class ProposalNet:
             _stream(stream)))
         return [Answer(float(r.value), (int(r.x), int(r.y)), float(r.margin), int(r.path), int(r.uncertified))
                 for r in res[:n]]
+
+
+def match_proposals(image: torch.Tensor, templates: torch.Tensor, origins: torch.Tensor, *,
+                    certify: bool = True, stream=None) -> list[Answer]:
+    """The verification, certification and fallback stages with proposals
+    from elsewhere (ipb_match_proposals_device): `origins` is a (t, k) int32
+    CUDA tensor of template origins y * (W - 47) + x, k <= 16 per template,
+    each the centre of a 32 x 32 window scored exactly. Same answers as
+    propose_and_match (exact SumOfSquaredErrors minima); margin is +inf."""
+    _u8(image, "image")
+    _u8(templates, "templates")
+    if templates.dim() != 3:
+        raise ValueError("templates must be a (t, h, w) tensor")
+    if origins.dtype != torch.int32 or not origins.is_cuda or origins.dim() != 2 or \
+            origins.shape[0] != templates.shape[0] or not origins.is_contiguous():
+        raise ValueError("origins must be a contiguous (t, k) int32 CUDA tensor")
+    H, W = image.shape
+    n, k = origins.shape
+    res = (ProposalResult * max(n, 1))()
+    opt = ProposeOptions(k, 0.1, int(certify))
+    check(_bind().ipb_match_proposals_device(
+        image.data_ptr(), W, H, templates.data_ptr(), templates.shape[2], templates.shape[1], n, 0,
+        origins.data_ptr(), k, C.byref(opt), res, _stream(stream)))
+    return [Answer(float(r.value), (int(r.x), int(r.y)), float(r.margin), int(r.path), int(r.uncertified))
+            for r in res[:n]]
+
+
+def pyramid_origins(image: torch.Tensor, templates: torch.Tensor, k: int = 16) -> torch.Tensor:
+    """Coarse-pyramid proposals, the baseline the network is compared with
+    (computed with torch operators; not a query path): SumOfSquaredErrors of
+    the 4x box-downsampled templates over the 4x box-downsampled image, the
+    best position of each 8 x 8 cell of that map, the k best cells per
+    template. Returns (t, k) int32 origins for match_proposals: 4x each
+    downsampled position, y * (W - 47) + x."""
+    import torch.nn.functional as F
+    H, W = image.shape
+    ds = F.avg_pool2d(image.float()[None, None], 4)
+    tds = F.avg_pool2d(templates.float()[:, None], 4)
+    cross = F.conv2d(ds, tds)[0]
+    sq = F.avg_pool2d(ds * ds, tds.shape[-1], stride=1)[0, 0] * float(tds.shape[-1] * tds.shape[-2])
+    sse = sq[None] - 2.0 * cross + (tds * tds).sum((1, 2, 3))[:, None, None]
+    T, Hm, Wm = sse.shape
+    vals, idx = F.max_pool2d(-sse[:, None], 8, stride=8, ceil_mode=True, return_indices=True)
+    top = vals.reshape(T, -1).topk(k, dim=1).indices
+    pos = idx.reshape(T, -1).gather(1, top)
+    qy, qx = pos // Wm, pos % Wm
+    Wo, Ho = W - templates.shape[2] + 1, H - templates.shape[1] + 1
+    ox, oy = (4 * qx).clamp(max=Wo - 1), (4 * qy).clamp(max=Ho - 1)
+    return (oy * Wo + ox).to(torch.int32).contiguous()
 
 
 # ---- training data ----------------------------------------------------------------

@@ -418,7 +418,7 @@ typedef struct ipb_proposal_result {
     uint32_t path;      /* 0: proposals, verified and certified; 1: fallback (low margin);
                            2: fallback (not certified) */
     uint32_t uncertified; /* blocks of 4 x 4 positions the certificate could not exclude
-                             outside the proposed windows (verified exactly when at most 512) */
+                             outside the proposed windows (verified exactly when at most 16384) */
 } ipb_proposal_result;
 
 /* Answers n_templates SumOfSquaredErrors queries of 48 x 48 templates
@@ -431,6 +431,19 @@ ipb_status ipb_propose_and_match_device(const ipb_proposal_net *net, const uint8
                                         uint32_t template_height, uint32_t n_templates, int method,
                                         const ipb_propose_options *options, ipb_proposal_result *results,
                                         void *stream);
+
+/* The same queries with the proposals given instead of the network's: k
+ * (1..16) template origins per template in d_origins (device, n_templates x k,
+ * y * (image_width - 47) + x), each the centre of a 32 x 32 window of
+ * positions scored exactly, then the same certification and exhaustive
+ * fallback (options: certify; top_k and min_margin are ignored, margins are
+ * +inf). Used to compare proposal sources on equal terms. */
+ipb_status ipb_match_proposals_device(const uint8_t *d_image, uint32_t image_width, uint32_t image_height,
+                                      const uint8_t *d_templates, uint32_t template_width,
+                                      uint32_t template_height, uint32_t n_templates, int method,
+                                      const uint32_t *d_origins, uint32_t k,
+                                      const ipb_propose_options *options, ipb_proposal_result *results,
+                                      void *stream);
 
 /* ---- find_extremes -------------------------------------------------------- */
 

@@ -144,6 +144,27 @@ def test_trained_network_gains_over_untrained():
     assert ok_t >= 0.8 and ok_t >= ok_u + 0.3, (ok_t, ok_u)
 
 
+def test_ablation_network_and_pyramid_proposals():
+    # the same verification, certification and fallback fed by the trained
+    # network (with the 0.1 margin gate, and with the certificate alone) or by
+    # coarse-pyramid proposals: every answer exact; dropping the margin gate
+    # only moves templates from the fallback to the certificate; the rates
+    # themselves are reported by bench.py (learned.ablation_pyramid)
+    import torch
+    image, templates, _ = synthetic.rect_scene(W=2048, H=2048, n_rects=60, n_templates=64, seed=79)
+    di, dt = torch.from_numpy(image).cuda(), torch.from_numpy(templates).cuda()
+    exact = _exact_answers(image, templates)
+    trained = learned.ProposalNet.trained()
+    net = trained.propose_and_match(di, dt)
+    net0 = trained.propose_and_match(di, dt, min_margin=0.0)
+    pyr = learned.match_proposals(di, dt, learned.pyramid_origins(di, dt))
+    for answers in (net, net0, pyr):
+        assert not _check_exact(answers, exact)
+    ok = [sum(a.path == 0 for a in answers) / 64 for answers in (net, net0, pyr)]
+    assert ok[1] >= ok[0] and min(ok) >= 0.8, ok
+    assert all(a.path in (0, 2) for a in net0 + pyr)  # no margin gate on these
+
+
 def test_rejects_unsupported_queries():
     import torch
     net = learned.ProposalNet(seed=1)
@@ -153,3 +174,6 @@ def test_rejects_unsupported_queries():
     with pytest.raises(ValueError, match="multiples of 32"):
         net.propose_and_match(torch.zeros((250, 256), dtype=torch.uint8, device="cuda"),
                               torch.zeros((2, 48, 48), dtype=torch.uint8, device="cuda"))
+    shifted = torch.zeros(256 * 256 + 16, dtype=torch.uint8, device="cuda")[1:1 + 256 * 256].view(256, 256)
+    with pytest.raises(ValueError, match="16-byte aligned"):
+        net.propose_and_match(shifted, torch.zeros((2, 48, 48), dtype=torch.uint8, device="cuda"))
