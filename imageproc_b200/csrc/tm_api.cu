@@ -209,6 +209,12 @@ struct Context {
   void* stage = nullptr;
   size_t stage_cap = 0;
   cudaEvent_t stage_free = nullptr;
+  // page-locked bounce buffer for pageable score maps of banded calls: each
+  // band's rows land there and the host copies them out while later bands
+  // are still computed and copied (band_out[b]: band b's rows have landed)
+  void* ostage = nullptr;
+  size_t ostage_cap = 0;
+  cudaEvent_t band_out[kMaxBands] = {};
   ~Context() {
     if (device < 0) return;
     cudaSetDevice(device);
@@ -222,6 +228,7 @@ struct Context {
       }
       if (band_in[b]) cudaEventDestroy(band_in[b]);
       if (band_done[b]) cudaEventDestroy(band_done[b]);
+      if (band_out[b]) cudaEventDestroy(band_out[b]);
     }
     if (out_done) cudaEventDestroy(out_done);
     if (stage_free) {
@@ -229,6 +236,7 @@ struct Context {
       cudaEventDestroy(stage_free);
     }
     if (stage) cudaFreeHost(stage);
+    if (ostage) cudaFreeHost(ostage);
     for (cudaStream_t s : {s_in, s_out})
       if (s) cudaStreamDestroy(s);
     for (DevBuf* b : {&scratch, &ext_scratch, &ext_result, &img, &tpl, &mask, &out, &errw, &many_keys, &rgb, &keys})
@@ -382,6 +390,8 @@ ipb_status ensure_band_streams(Context* c, uint32_t nb) {
     if (!c->band_in[b]) IPB_CUDA(cudaEventCreateWithFlags(&c->band_in[b], cudaEventDisableTiming), "cudaEventCreate");
     if (!c->band_done[b])
       IPB_CUDA(cudaEventCreateWithFlags(&c->band_done[b], cudaEventDisableTiming), "cudaEventCreate");
+    if (!c->band_out[b])
+      IPB_CUDA(cudaEventCreateWithFlags(&c->band_out[b], cudaEventDisableTiming), "cudaEventCreate");
   }
   if (!c->out_done) IPB_CUDA(cudaEventCreateWithFlags(&c->out_done, cudaEventDisableTiming), "cudaEventCreate");
   return IPB_OK;
@@ -483,13 +493,15 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
   if (side_by_side && (st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
   // A copy into page-locked memory returns at once, so a band's score rows are
   // queued as soon as its launch is: they cross while the host still copies
-  // later image rows from pageable memory (which holds the calling thread).
-  // Into pageable memory the copy would hold the thread too: queued last.
+  // later image rows. A pageable score map is reached through the output
+  // bounce buffer, which the host drains band by band at the end.
   const bool out_locked = host_memory_is_locked(out);
   const uint32_t W = full.W, Wo = full.W - full.w + 1, Ho = full.H - full.h + 1;
   // a pageable image goes through the context's page-locked bounce buffer
   const size_t ib = (size_t)W * full.H;
-  const bool staged = ib > 0 && !host_memory_is_locked(image);
+  // (below 16 MiB the driver's own staging of a pageable copy is faster than
+  // waking the copy threads band by band)
+  const bool staged = ib >= (size_t(16) << 20) && !host_memory_is_locked(image);
   if (staged) {
     if (c->stage_free) IPB_CUDA(cudaEventSynchronize(c->stage_free), "cudaEventSynchronize");
     if (c->stage_cap < ib) {
@@ -501,6 +513,17 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
     }
     if (!c->stage_free) IPB_CUDA(cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming), "cudaEventCreate");
   }
+  // a pageable score map goes through the page-locked output bounce buffer
+  const size_t ob = (size_t)Wo * Ho * sizeof(float);
+  const bool ostaged = !out_locked && ob > 0;
+  if (ostaged && c->ostage_cap < ob) {
+    if (c->ostage) cudaFreeHost(c->ostage);
+    c->ostage = nullptr;
+    c->ostage_cap = 0;
+    IPB_CUDA(cudaMallocHost(&c->ostage, align_up(ob, 1 << 20)), "cudaMallocHost (score staging)");
+    c->ostage_cap = align_up(ob, 1 << 20);
+  }
+  float* dst_out = ostaged ? static_cast<float*>(c->ostage) : out;
   const uint8_t* src_img = staged ? static_cast<const uint8_t*>(c->stage) : image;
   const size_t tb = (size_t)full.w * full.h;
   const uint32_t rows = (uint32_t)align_up((Ho + nb - 1) / nb, 16);
@@ -508,9 +531,10 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
   auto queue_out = [&](uint32_t b) -> ipb_status {
     const uint32_t o0 = b * rows, o1 = std::min(Ho, o0 + rows);
     IPB_CUDA(cudaStreamWaitEvent(c->s_out, c->band_done[b], 0), "cudaStreamWaitEvent");
-    IPB_CUDA(cudaMemcpyAsync(out + (size_t)o0 * Wo, full.out + (size_t)o0 * Wo, (size_t)(o1 - o0) * Wo * sizeof(float),
-                             cudaMemcpyDeviceToHost, c->s_out),
+    IPB_CUDA(cudaMemcpyAsync(dst_out + (size_t)o0 * Wo, full.out + (size_t)o0 * Wo,
+                             (size_t)(o1 - o0) * Wo * sizeof(float), cudaMemcpyDeviceToHost, c->s_out),
              "copy score rows");
+    IPB_CUDA(cudaEventRecord(c->band_out[b], c->s_out), "cudaEventRecord");
     return IPB_OK;
   };
   auto enqueue = [&]() -> ipb_status {
@@ -550,14 +574,21 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
         if (s2) return s2;
       }
       IPB_CUDA(cudaEventRecord(c->band_done[bands], a.stream), "cudaEventRecord");
-      if (out_locked && (st = queue_out(bands))) return st;
+      if ((st = queue_out(bands))) return st;
     }
     if (staged) IPB_CUDA(cudaEventRecord(c->stage_free, c->s_in), "cudaEventRecord");
-    if (!out_locked)
-      for (uint32_t b = 0; b < bands; ++b)
-        if ((st = queue_out(b))) return st;
     IPB_CUDA(cudaEventRecord(c->out_done, c->s_out), "cudaEventRecord");
     IPB_CUDA(cudaStreamWaitEvent(c->stream, c->out_done, 0), "cudaStreamWaitEvent");
+    if (ostaged)
+      // each band's rows to the caller's buffer as soon as they have landed,
+      // while later bands are still in flight
+      for (uint32_t b = 0; b < bands; ++b) {
+        IPB_CUDA(cudaEventSynchronize(c->band_out[b]), "cudaEventSynchronize");
+        const uint32_t o0 = b * rows, o1 = std::min(Ho, o0 + rows);
+        CopyPool::get().copy(reinterpret_cast<uint8_t*>(out + (size_t)o0 * Wo),
+                             reinterpret_cast<const uint8_t*>(dst_out + (size_t)o0 * Wo),
+                             (size_t)(o1 - o0) * Wo * sizeof(float));
+      }
     return IPB_OK;
   };
   if ((st = enqueue())) {

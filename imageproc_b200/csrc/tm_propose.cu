@@ -529,96 +529,162 @@ __device__ __forceinline__ unsigned long long lb_term(uint32_t st, uint32_t pack
 }
 
 constexpr int kCertSlices = 16;  // blocks of threads per template
+constexpr uint32_t kMaxLevel2 = 65536;  // most 16 x 16 blocks a template may carry to the last level
 
-// Grid (template, slice): each block takes every kCertSlices-th block of
-// 64 x 64 positions. A block whose lower bound exceeds the verified minimum is
-// excluded; the others split into 16 blocks of 16 x 16, and those into 16
-// micro blocks of 4 x 4 positions. A micro block that is neither excluded nor
-// inside a verified window is appended to the template's extra list (counter
-// n_extra[t], zeroed by windows_kernel); a count above kMaxExtra means the
-// template falls back.
-__global__ void __launch_bounds__(256) certify_kernel(const uint8_t* __restrict__ tpl, const TopK* __restrict__ tk,
-                                                      float min_margin, const unsigned long long* __restrict__ best,
-                                                      const uint32_t* __restrict__ micro,
-                                                      const uint32_t* __restrict__ span4,
-                                                      const uint32_t* __restrict__ span16, uint32_t Mx, uint32_t My,
-                                                      uint32_t Wo, uint32_t Ho, const Rect* __restrict__ wins,
-                                                      const uint32_t* __restrict__ nwin, uint32_t max_rects,
-                                                      uint32_t* __restrict__ extra, uint32_t* __restrict__ n_extra) {
-  __shared__ uint32_t s_st[16];
-  __shared__ Rect s_win[kMaxTopK];
-  const uint32_t t = blockIdx.x;
-  if (tk[t].margin < min_margin || tk[t].count == 0) return;
-  const uint8_t* tp = tpl + (size_t)t * kTpl * kTpl;
+// What the three certification levels share: the template's 16 block sums,
+// the verified minimum, and the lower bound of a block of positions starting
+// at micro block (px, py), template block b at micro offset 3 b, from a table.
+struct CertCtx {
+  uint32_t st[16];
+  float sstar;
+  bool skip;  // low margin: the template falls back without a certificate
+};
+
+__device__ __forceinline__ void cert_setup(CertCtx& cc, uint32_t* s_st, const uint8_t* tpl, const TopK& tk,
+                                           float min_margin, unsigned long long best) {
   if (threadIdx.x < 16) {
+    const uint8_t* tp = tpl;
     const uint32_t by = threadIdx.x >> 2, bx = threadIdx.x & 3;
     uint32_t s = 0;
     for (int dy = 0; dy < kBlk; ++dy)
       for (int dx = 0; dx < kBlk; ++dx) s += tp[(by * kBlk + dy) * kTpl + bx * kBlk + dx];
     s_st[threadIdx.x] = s;
   }
-  const uint32_t nw = nwin[t];
-  if (threadIdx.x < nw) s_win[threadIdx.x] = wins[(size_t)t * max_rects + threadIdx.x];
   __syncthreads();
-  // the verified minimum; a block is excluded when RN_f32(ceil(LB)) > it
-  const float sstar = okey_value((uint32_t)(best[t] >> 32));
-  auto excluded = [&](unsigned long long num) {
-    const unsigned long long lb = (num + 143ull) / 144ull;  // SSE is an integer >= num / 144
-    return (float)lb > sstar;
-  };
-  // lower bound of a block of positions starting at micro block (px, py),
-  // template block b at micro offset 3 * b, from `table`
-  auto bound = [&](const uint32_t* table, uint32_t px, uint32_t py) {
-    unsigned long long num = 0ull;
 #pragma unroll
-    for (int b = 0; b < 16; ++b) {
-      const uint32_t mx = px + 3 * (b & 3), my = py + 3 * (b >> 2);
-      if (mx < Mx && my < My) num += lb_term(s_st[b], table[(size_t)my * Mx + mx]);
-    }
-    return num;
-  };
-  const uint32_t Pmx = (Wo + 3) / 4, Pmy = (Ho + 3) / 4;  // micro blocks of positions
+  for (int b = 0; b < 16; ++b) cc.st[b] = s_st[b];
+  cc.sstar = okey_value((uint32_t)(best >> 32));
+  cc.skip = tk.margin < min_margin || tk.count == 0;
+}
+
+__device__ __forceinline__ bool cert_excluded(const CertCtx& cc, const uint32_t* __restrict__ table, uint32_t Mx,
+                                              uint32_t My, uint32_t px, uint32_t py) {
+  unsigned long long num = 0ull;
+#pragma unroll
+  for (int b = 0; b < 16; ++b) {
+    const uint32_t mx = px + 3 * (b & 3), my = py + 3 * (b >> 2);
+    if (mx < Mx && my < My) num += lb_term(cc.st[b], __ldg(table + (size_t)my * Mx + mx));
+  }
+  // SSE is an integer >= num / 144; excluded when RN_f32(ceil(LB)) exceeds the minimum
+  return (float)((num + 143ull) / 144ull) > cc.sstar;
+}
+
+// Level 1, grid (template, slice): every block of 64 x 64 positions (16 x 16
+// micro blocks) whose bound does not exclude it goes to list1.
+__global__ void __launch_bounds__(256) certify_l1_kernel(const uint8_t* __restrict__ tpl,
+                                                         const TopK* __restrict__ tk, float min_margin,
+                                                         const unsigned long long* __restrict__ best,
+                                                         const uint32_t* __restrict__ span16, uint32_t Mx,
+                                                         uint32_t My, uint32_t Pmx, uint32_t Pmy,
+                                                         uint32_t* __restrict__ list1, uint32_t cap1,
+                                                         uint32_t* __restrict__ n1) {
+  __shared__ uint32_t s_st[16];
+  const uint32_t t = blockIdx.x;
+  CertCtx cc;
+  cert_setup(cc, s_st, tpl + (size_t)t * kTpl * kTpl, tk[t], min_margin, best[t]);
+  if (cc.skip) return;
   const uint32_t C3x = (Pmx + 15) / 16, C3y = (Pmy + 15) / 16;
   for (uint32_t q = blockIdx.y * blockDim.x + threadIdx.x; q < C3x * C3y; q += gridDim.y * blockDim.x) {
-    const uint32_t p3x = 16 * (q % C3x), p3y = 16 * (q / C3x);
-    if (excluded(bound(span16, p3x, p3y))) continue;
-    for (uint32_t k2 = 0; k2 < 16; ++k2) {
-      const uint32_t p2x = p3x + 4 * (k2 & 3), p2y = p3y + 4 * (k2 >> 2);
-      if (p2x >= Pmx || p2y >= Pmy || excluded(bound(span4, p2x, p2y))) continue;
-      for (uint32_t k1 = 0; k1 < 16; ++k1) {
-        const uint32_t px = p2x + (k1 & 3), py = p2y + (k1 >> 2);
-        if (px >= Pmx || py >= Pmy || excluded(bound(micro, px, py))) continue;
-        const uint32_t x0 = 4 * px, y0 = 4 * py;
-        const uint32_t x1 = min(x0 + 4, Wo), y1 = min(y0 + 4, Ho);
-        bool covered = false;
-        for (uint32_t w = 0; w < nw && !covered; ++w) {
-          const Rect r = s_win[w];
-          covered = x0 >= r.x0 && y0 >= r.y0 && x1 <= r.x0 + r.w && y1 <= r.y0 + r.h;
-        }
-        if (covered) continue;
-        const uint32_t slot = atomicAdd(n_extra + t, 1u);
-        if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = py * Pmx + px;
-      }
+    const uint32_t px = 16 * (q % C3x), py = 16 * (q / C3x);
+    if (cert_excluded(cc, span16, Mx, My, px, py)) continue;
+    const uint32_t slot = atomicAdd(n1 + t, 1u);
+    if (slot < cap1) list1[(size_t)t * cap1 + slot] = q;  // cap1 = C3x * C3y: never exceeded
+  }
+}
+
+// Level 2: the 16 blocks of 16 x 16 positions inside each list1 entry; the
+// ones not excluded go to list2 (more than kMaxLevel2: the template falls
+// back, recorded as an extra count above kMaxExtra).
+__global__ void __launch_bounds__(256) certify_l2_kernel(const uint8_t* __restrict__ tpl,
+                                                         const TopK* __restrict__ tk, float min_margin,
+                                                         const unsigned long long* __restrict__ best,
+                                                         const uint32_t* __restrict__ span4, uint32_t Mx,
+                                                         uint32_t My, uint32_t Pmx, uint32_t Pmy,
+                                                         const uint32_t* __restrict__ list1, uint32_t cap1,
+                                                         const uint32_t* __restrict__ n1,
+                                                         uint32_t* __restrict__ list2, uint32_t* __restrict__ n2,
+                                                         uint32_t* __restrict__ n_extra) {
+  __shared__ uint32_t s_st[16];
+  const uint32_t t = blockIdx.x;
+  CertCtx cc;
+  cert_setup(cc, s_st, tpl + (size_t)t * kTpl * kTpl, tk[t], min_margin, best[t]);
+  if (cc.skip) return;
+  const uint32_t C3x = (Pmx + 15) / 16;
+  const uint32_t work = min(n1[t], cap1) * 16u;
+  for (uint32_t e = blockIdx.y * blockDim.x + threadIdx.x; e < work; e += gridDim.y * blockDim.x) {
+    const uint32_t q = list1[(size_t)t * cap1 + (e >> 4)], k2 = e & 15u;
+    const uint32_t px = 16 * (q % C3x) + 4 * (k2 & 3), py = 16 * (q / C3x) + 4 * (k2 >> 2);
+    if (px >= Pmx || py >= Pmy || cert_excluded(cc, span4, Mx, My, px, py)) continue;
+    const uint32_t slot = atomicAdd(n2 + t, 1u);
+    if (slot < kMaxLevel2)
+      list2[(size_t)t * kMaxLevel2 + slot] = py * Pmx + px;
+    else
+      atomicMax(n_extra + t, (uint32_t)kMaxExtra + 1u);
+  }
+}
+
+// Level 3: the 16 micro blocks (4 x 4 positions) inside each list2 entry. A
+// micro block that is neither excluded nor inside a verified window is
+// appended to the template's extra list (counter n_extra[t]); a count above
+// kMaxExtra means the template falls back.
+__global__ void __launch_bounds__(256) certify_l3_kernel(const uint8_t* __restrict__ tpl,
+                                                         const TopK* __restrict__ tk, float min_margin,
+                                                         const unsigned long long* __restrict__ best,
+                                                         const uint32_t* __restrict__ micro, uint32_t Mx,
+                                                         uint32_t My, uint32_t Pmx, uint32_t Pmy, uint32_t Wo,
+                                                         uint32_t Ho, const uint32_t* __restrict__ list2,
+                                                         const uint32_t* __restrict__ n2,
+                                                         const Rect* __restrict__ wins,
+                                                         const uint32_t* __restrict__ nwin, uint32_t max_rects,
+                                                         uint32_t* __restrict__ extra, uint32_t* __restrict__ n_extra) {
+  __shared__ uint32_t s_st[16];
+  __shared__ Rect s_win[kMaxTopK];
+  const uint32_t t = blockIdx.x;
+  const uint32_t nw = nwin[t];
+  if (threadIdx.x < nw) s_win[threadIdx.x] = wins[(size_t)t * max_rects + threadIdx.x];
+  CertCtx cc;
+  cert_setup(cc, s_st, tpl + (size_t)t * kTpl * kTpl, tk[t], min_margin, best[t]);  // syncs s_win too
+  if (cc.skip || n_extra[t] > (uint32_t)kMaxExtra) return;
+  const uint32_t work = min(n2[t], kMaxLevel2) * 16u;
+  for (uint32_t e = blockIdx.y * blockDim.x + threadIdx.x; e < work; e += gridDim.y * blockDim.x) {
+    const uint32_t p2 = list2[(size_t)t * kMaxLevel2 + (e >> 4)], k1 = e & 15u;
+    const uint32_t px = p2 % Pmx + (k1 & 3), py = p2 / Pmx + (k1 >> 2);
+    if (px >= Pmx || py >= Pmy || cert_excluded(cc, micro, Mx, My, px, py)) continue;
+    const uint32_t x0 = 4 * px, y0 = 4 * py;
+    const uint32_t x1 = min(x0 + 4, Wo), y1 = min(y0 + 4, Ho);
+    bool covered = false;
+    for (uint32_t w = 0; w < nw && !covered; ++w) {
+      const Rect r = s_win[w];
+      covered = x0 >= r.x0 && y0 >= r.y0 && x1 <= r.x0 + r.w && y1 <= r.y0 + r.h;
     }
+    if (covered) continue;
+    const uint32_t slot = atomicAdd(n_extra + t, 1u);
+    if (slot < kMaxExtra) extra[(size_t)t * kMaxExtra + slot] = py * Pmx + px;
   }
 }
 
 // Exact minimum over the extra blocks of 4 x 4 positions (packed micro-block
 // indices py * Pmx + px from certify_kernel), every block of every template
-// whose list fits: grid (slices, template), one warp per block, lanes = 16
-// positions x 2 halves of the template's rows. Each lane sums X = sum I*T and
-// Y = sum I^2 over its 24 rows with dp4a on aligned image words (read through
-// the cache; W * H is a multiple of 4, so no word crosses the image's end)
-// shifted by byte_perm, the halves meet through one shuffle, and SSE =
-// Y - 2X + TSS rounds once to f32 as in verify_kernel. The first minimum goes
-// to best[t].
-__global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __restrict__ img, uint32_t W,
+// whose list fits: grid (slices, template), one warp per block. The warp
+// stages the block's image patch (51 rows x 13 words; W is a multiple of 32
+// and 4 px is a multiple of 4, so the words are aligned; words past the
+// image read as zero, and feed no valid position) in its own shared memory,
+// then: R(r, ox) = sum of I^2 over 48 bytes of patch row r from column ox
+// (51 x 4 sums, dp4a), Y(ox, oy) = sum over 48 rows of R; X by lanes = 16
+// positions x 2 halves of the template's rows, dp4a on byte_perm-shifted
+// patch words; the halves meet through one shuffle and SSE = Y - 2X + TSS
+// rounds once to f32 as in verify_kernel. The first minimum goes to best[t].
+constexpr int kPatchRows = 4 + kTpl - 1;        // 51
+constexpr int kPatchWords = (4 + kTpl + 3) / 4;  // 13 (52 bytes >= 51)
+__global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
                                                             const uint8_t* __restrict__ tpl,
                                                             const uint32_t* __restrict__ extra,
                                                             const uint32_t* __restrict__ n_extra, uint32_t Pmx,
                                                             uint32_t Wo, uint32_t Ho,
                                                             unsigned long long* __restrict__ best) {
   __shared__ uint32_t s_tpl[kTpl][kTpl / 4 + 1];  // padded: the two row halves fall in different banks
+  __shared__ uint32_t s_patch[8][kPatchRows][kPatchWords];
+  __shared__ uint32_t s_rsq[8][kPatchRows][4];
   __shared__ unsigned long long s_tss[8];
   __shared__ unsigned long long s_best[8];
   const uint32_t t = blockIdx.y;
@@ -639,33 +705,55 @@ __global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __res
   for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tss += s_tss[k];
   const uint32_t pos = lane & 15u, half = lane >> 4;
   const uint32_t ox = pos & 3u, oy = pos >> 2;
+  const uint32_t sel = 0x3210u + ox * 0x1111u;
   unsigned long long mykey = ~0ull;
   const uint32_t* const img32 = reinterpret_cast<const uint32_t*>(img);
+  const uint32_t wpr = W / 4;  // words per image row
+  uint32_t (*patch)[kPatchWords] = s_patch[warp];
+  uint32_t (*rsq)[4] = s_rsq[warp];
   for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + warp; i < n; i += gridDim.x * (blockDim.x >> 5)) {
     const uint32_t mb = extra[(size_t)t * kMaxExtra + i];
-    const uint32_t x = 4 * (mb % Pmx) + ox, y = 4 * (mb / Pmx) + oy;
-    const bool valid = x < Wo && y < Ho;
-    const uint32_t xs = valid ? x : 0u, ys = valid ? y : 0u;  // in-bounds reads for the block's edge lanes
+    const uint32_t x0 = 4 * (mb % Pmx), y0 = 4 * (mb / Pmx);
+    __syncwarp();  // the previous block's reads of the patch are done
+    for (uint32_t e = lane; e < (uint32_t)(kPatchRows * kPatchWords); e += 32) {
+      const uint32_t r = e / kPatchWords, c = e % kPatchWords;
+      const uint32_t y = y0 + r, xw = x0 / 4 + c;
+      patch[r][c] = (y < H && xw < wpr) ? __ldg(img32 + (size_t)y * wpr + xw) : 0u;
+    }
+    __syncwarp();
+    // R(r, ox): squares of 48 bytes of row r from column ox
+    for (uint32_t e = lane; e < (uint32_t)(kPatchRows * 4); e += 32) {
+      const uint32_t r = e >> 2, o = e & 3u;
+      const uint32_t sl = 0x3210u + o * 0x1111u;
+      uint32_t acc = 0u, cur = patch[r][0];
+#pragma unroll
+      for (int k = 0; k < kTpl / 4; ++k) {
+        const uint32_t nxt = patch[r][k + 1];
+        const uint32_t iw = __byte_perm(cur, nxt, sl);
+        acc = __dp4a(iw, iw, acc);
+        cur = nxt;
+      }
+      rsq[r][o] = acc;
+    }
     uint32_t X = 0u, Y = 0u;
 #pragma unroll 2
     for (uint32_t dy = half * (kTpl / 2); dy < (half + 1) * (kTpl / 2); ++dy) {
-      const size_t a = (size_t)(ys + dy) * W + xs;
-      const uint32_t* row = img32 + (a >> 2);
-      const uint32_t sel = 0x3210u + (uint32_t)(a & 3u) * 0x1111u;
-      uint32_t cur = __ldg(row);
+      const uint32_t* prow = patch[oy + dy];
+      uint32_t cur = prow[0];
 #pragma unroll
       for (int k = 0; k < kTpl / 4; ++k) {
-        // the word after the window's last byte is read only when the window is unaligned
-        const uint32_t nxt = (k + 1 < kTpl / 4 || (a & 3u)) ? __ldg(row + k + 1) : 0u;
-        const uint32_t iw = __byte_perm(cur, nxt, sel);
-        X = __dp4a(iw, s_tpl[dy][k], X);
-        Y = __dp4a(iw, iw, Y);
+        const uint32_t nxt = prow[k + 1];
+        X = __dp4a(__byte_perm(cur, nxt, sel), s_tpl[dy][k], X);
         cur = nxt;
       }
     }
+    __syncwarp();  // the square sums are written
+#pragma unroll 4
+    for (uint32_t dy = half * (kTpl / 2); dy < (half + 1) * (kTpl / 2); ++dy) Y += rsq[oy + dy][ox];
     X += __shfl_xor_sync(0xffffffffu, X, 16);
     Y += __shfl_xor_sync(0xffffffffu, Y, 16);
-    if (valid && half == 0) {
+    const uint32_t x = x0 + ox, y = y0 + oy;
+    if (x < Wo && y < Ho && half == 0) {
       const unsigned long long sse = (unsigned long long)Y + tss - 2ull * X;
       const float score = (float)sse;  // round to nearest
       const unsigned long long key = ((unsigned long long)okey(score) << 32) | (y * Wo + x);
@@ -779,6 +867,10 @@ struct Carve {
   uint32_t* nwin;
   uint32_t* extra;  // per template: kMaxExtra packed micro-block indices
   uint32_t* n_extra;
+  uint32_t* list1;  // certification work lists: per template cap1 64 x 64 blocks,
+  uint32_t* list2;  // kMaxLevel2 16 x 16 blocks,
+  uint32_t* n12;    // and their counts (n1: T words, then n2: T words)
+  uint32_t cap1;
   unsigned long long* best;
   uint32_t* micro;
   uint32_t* span4;
@@ -814,6 +906,13 @@ Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
   c.nwin = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
   c.extra = reinterpret_cast<uint32_t*>(take((size_t)T * kMaxExtra * sizeof(uint32_t)));
   c.n_extra = reinterpret_cast<uint32_t*>(take((size_t)T * 4));
+  {
+    const uint32_t Pmx = (W - kTpl + 1 + 3) / 4, Pmy = (H - kTpl + 1 + 3) / 4;
+    c.cap1 = ((Pmx + 15) / 16) * ((Pmy + 15) / 16);
+  }
+  c.list1 = reinterpret_cast<uint32_t*>(take((size_t)T * c.cap1 * 4));
+  c.list2 = reinterpret_cast<uint32_t*>(take((size_t)T * kMaxLevel2 * 4));
+  c.n12 = reinterpret_cast<uint32_t*>(take((size_t)T * 8));
   c.best = reinterpret_cast<unsigned long long*>(take((size_t)T * 8));
   const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
   c.micro = reinterpret_cast<uint32_t*>(take((size_t)Mx * My * 4));
@@ -903,11 +1002,20 @@ ipb_status finish_queries(ProposeScratch& ps, const Carve& c, unsigned int call_
     count_launch(kKernelPropose);
     span_table_kernel<<<(Mx * My + 255) / 256, 256, 0, s>>>(c.span4, Mx, My, 4, c.span16);
     count_launch(kKernelPropose);
-    certify_kernel<<<dim3(T, kCertSlices), 256, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.micro, c.span4,
-                                                        c.span16, Mx, My, Wo, Ho, c.wins, c.nwin, opt.top_k,
-                                                        c.extra, c.n_extra);
+    const uint32_t Pmx = (Wo + 3) / 4, Pmy = (Ho + 3) / 4;
+    P_CUDA(cudaMemsetAsync(c.n12, 0, (size_t)T * 8, s), "certification counters");
+    certify_l1_kernel<<<dim3(T, kCertSlices), 256, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.span16, Mx, My,
+                                                           Pmx, Pmy, c.list1, c.cap1, c.n12);
     count_launch(kKernelPropose);
-    verify_blocks_kernel<<<dim3(kVerifySlices, T), 256, 0, s>>>(d_image, W, d_templates, c.extra, c.n_extra,
+    certify_l2_kernel<<<dim3(T, kCertSlices), 256, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.span4, Mx, My,
+                                                           Pmx, Pmy, c.list1, c.cap1, c.n12, c.list2, c.n12 + T,
+                                                           c.n_extra);
+    count_launch(kKernelPropose);
+    certify_l3_kernel<<<dim3(T, 4 * kCertSlices), 256, 0, s>>>(d_templates, c.tk, opt.min_margin, c.best, c.micro,
+                                                               Mx, My, Pmx, Pmy, Wo, Ho, c.list2, c.n12 + T, c.wins,
+                                                               c.nwin, opt.top_k, c.extra, c.n_extra);
+    count_launch(kKernelPropose);
+    verify_blocks_kernel<<<dim3(kVerifySlices, T), 256, 0, s>>>(d_image, W, H, d_templates, c.extra, c.n_extra,
                                                                    (Wo + 3) / 4, Wo, Ho, c.best);
     count_launch(kKernelPropose);
     P_CUDA(cudaGetLastError(), "certification");
