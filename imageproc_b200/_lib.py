@@ -121,8 +121,6 @@ def tensor_plan(w: int, h: int, masked: bool, batch: bool) -> dict | None:
 
 _lib = None
 
-u8p = C.POINTER(C.c_uint8)
-f32p = C.POINTER(C.c_float)
 u32 = C.c_uint32
 
 
@@ -146,12 +144,15 @@ def lib() -> C.CDLL:
     L.ipb_profile_enable.argtypes = [C.c_int]
     L.ipb_profile_collect.argtypes = [C.POINTER(KernelStats), C.c_int]
     L.ipb_profile_collect.restype = C.c_int
-    host = [u8p, u32, u32, u8p, u32, u32, C.c_int]
+    # host buffers go in as plain addresses (numpy's .ctypes.data): building
+    # a typed ctypes pointer per argument costs microseconds per call
+    vp = C.c_void_p
+    host = [vp, u32, u32, vp, u32, u32, C.c_int]
     for name in ("ipb_match_template", "ipb_match_template_parallel"):
-        getattr(L, name).argtypes = host + [f32p]
+        getattr(L, name).argtypes = host + [vp]
         getattr(L, name).restype = C.c_int
     for name in ("ipb_match_template_with_mask", "ipb_match_template_with_mask_parallel"):
-        getattr(L, name).argtypes = host + [u8p, u32, u32, f32p]
+        getattr(L, name).argtypes = host + [vp, u32, u32, vp]
         getattr(L, name).restype = C.c_int
     L.ipb_match_template_device.argtypes = [
         C.c_void_p, u32, u32, C.c_void_p, u32, u32, C.c_void_p, u32, u32, C.c_int, C.c_int,

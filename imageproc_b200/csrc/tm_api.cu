@@ -7,6 +7,7 @@
 // stream before touching scratch and records it afterwards, so calls from one
 // thread on different streams never overlap on shared scratch.
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdio>
 #include <thread>
@@ -412,7 +413,10 @@ ipb_status ensure_band_streams(Context* c, uint32_t nb) {
 // engines directly: the driver would stage it through its own buffer at one
 // thread's memcpy rate while holding the calling thread. Copying it into a
 // page-locked buffer in parallel, band by band, lets each band's DMA start
-// while the next band's rows are still being copied.
+// while the next band's rows are still being copied. The workers spin on the
+// job generation for a short while after their last job (calls come in
+// bursts; a sleeping thread takes tens of microseconds to wake), then sleep
+// on a condition variable. One batch of jobs at a time.
 class CopyPool {
  public:
   static CopyPool& get() {
@@ -420,28 +424,37 @@ class CopyPool {
     return pool;
   }
   void copy(uint8_t* dst, const uint8_t* src, size_t n) {
-    const size_t parts = n >= (size_t(1) << 19) ? workers_.size() + 1 : 1;
+    const size_t parts = (n >= (size_t(1) << 18) && !workers_.empty()) ? workers_.size() + 1 : 1;
     if (parts == 1) {
       std::memcpy(dst, src, n);
       return;
     }
+    std::lock_guard<std::mutex> batch(batch_mu_);
     const size_t chunk = align_up((n + parts - 1) / parts, 4096);
-    std::unique_lock<std::mutex> lk(mu_);
-    size_t off = chunk;  // the caller copies [0, chunk)
-    for (; off < n; off += chunk) jobs_.push_back({dst + off, src + off, std::min(chunk, n - off)});
-    pending_ += jobs_.size();
-    lk.unlock();
-    cv_.notify_all();
+    uint32_t nj = 0;
+    for (size_t off = chunk; off < n && nj < kMaxJobs; off += chunk)
+      jobs_[nj++] = Job{dst + off, src + off, std::min(chunk, n - off)};
+    njobs_.store(nj, std::memory_order_relaxed);
+    pending_.store(nj, std::memory_order_relaxed);
+    const uint64_t g = ++gen_;
+    // publishes the jobs: a claim carries its batch's generation, so a worker
+    // still holding an older generation takes nothing from this batch
+    claim_.store(g << 32, std::memory_order_release);
+    if (sleepers_.load(std::memory_order_acquire) > 0) {
+      std::lock_guard<std::mutex> lk(mu_);
+      cv_.notify_all();
+    }
     std::memcpy(dst, src, std::min(chunk, n));
-    lk.lock();
-    done_.wait(lk, [&] { return pending_ == 0; });
+    run_jobs(g);  // help with what the workers have not taken yet
+    while (pending_.load(std::memory_order_acquire) != 0) {
+    }
   }
   ~CopyPool() {
+    stop_.store(true, std::memory_order_release);
     {
-      std::lock_guard<std::mutex> g(mu_);
-      stop_ = true;
+      std::lock_guard<std::mutex> lk(mu_);
+      cv_.notify_all();
     }
-    cv_.notify_all();
     for (std::thread& t : workers_) t.join();
   }
 
@@ -451,29 +464,52 @@ class CopyPool {
     const uint8_t* src;
     size_t n;
   };
+  static constexpr uint32_t kMaxJobs = 8;
   CopyPool() {
     const unsigned hw = std::thread::hardware_concurrency();
     const unsigned n = hw >= 8 ? 3u : (hw >= 4 ? 1u : 0u);
     for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this] { run(); });
   }
-  void run() {
-    std::unique_lock<std::mutex> lk(mu_);
+  // Takes jobs of batch g until none is left (or a newer batch replaced it).
+  void run_jobs(uint64_t g) {
+    uint64_t c = claim_.load(std::memory_order_acquire);
     for (;;) {
-      cv_.wait(lk, [&] { return stop_ || !jobs_.empty(); });
-      if (stop_) return;
-      const Job j = jobs_.front();
-      jobs_.pop_front();
-      lk.unlock();
+      if ((c >> 32) != g || (uint32_t)c >= njobs_.load(std::memory_order_relaxed)) return;
+      if (!claim_.compare_exchange_weak(c, c + 1, std::memory_order_acq_rel, std::memory_order_acquire)) continue;
+      const Job& j = jobs_[(uint32_t)c];
       std::memcpy(j.dst, j.src, j.n);
-      lk.lock();
-      if (--pending_ == 0) done_.notify_all();
+      pending_.fetch_sub(1, std::memory_order_release);
+      c = claim_.load(std::memory_order_acquire);
     }
   }
-  std::mutex mu_;
-  std::condition_variable cv_, done_;
-  std::deque<Job> jobs_;
-  size_t pending_ = 0;
-  bool stop_ = false;
+  void run() {
+    uint64_t seen = 0;
+    while (!stop_.load(std::memory_order_acquire)) {
+      const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(500);
+      uint64_t g = claim_.load(std::memory_order_acquire) >> 32;
+      while (g == seen && !stop_.load(std::memory_order_relaxed) && std::chrono::steady_clock::now() < spin_until)
+        g = claim_.load(std::memory_order_acquire) >> 32;
+      if (g == seen) {
+        std::unique_lock<std::mutex> lk(mu_);
+        sleepers_.fetch_add(1, std::memory_order_acq_rel);
+        cv_.wait(lk, [&] {
+          return stop_.load(std::memory_order_acquire) || (claim_.load(std::memory_order_acquire) >> 32) != seen;
+        });
+        sleepers_.fetch_sub(1, std::memory_order_acq_rel);
+        continue;
+      }
+      seen = g;
+      run_jobs(g);
+    }
+  }
+  std::mutex batch_mu_, mu_;
+  std::condition_variable cv_;
+  Job jobs_[kMaxJobs];
+  std::atomic<uint32_t> njobs_{0};
+  uint64_t gen_ = 0;
+  std::atomic<uint64_t> claim_{0};  // generation << 32 | next job
+  std::atomic<uint32_t> pending_{0}, sleepers_{0};
+  std::atomic<bool> stop_{false};
   std::vector<std::thread> workers_;
 };
 
@@ -499,9 +535,7 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
   const uint32_t W = full.W, Wo = full.W - full.w + 1, Ho = full.H - full.h + 1;
   // a pageable image goes through the context's page-locked bounce buffer
   const size_t ib = (size_t)W * full.H;
-  // (below 16 MiB the driver's own staging of a pageable copy is faster than
-  // waking the copy threads band by band)
-  const bool staged = ib >= (size_t(16) << 20) && !host_memory_is_locked(image);
+  const bool staged = ib >= (size_t(1) << 20) && !host_memory_is_locked(image);
   if (staged) {
     if (c->stage_free) IPB_CUDA(cudaEventSynchronize(c->stage_free), "cudaEventSynchronize");
     if (c->stage_cap < ib) {

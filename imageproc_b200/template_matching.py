@@ -92,8 +92,8 @@ def _gray(img: np.ndarray, what: str) -> np.ndarray:
     return np.ascontiguousarray(a)
 
 
-def _ptr(a: np.ndarray, ctype):
-    return a.ctypes.data_as(C.POINTER(ctype))
+def _ptr(a: np.ndarray):
+    return a.ctypes.data if a.size else None
 
 
 def _run(fn_name: str, image, template, method, mask=None) -> np.ndarray:
@@ -111,13 +111,11 @@ def _run(fn_name: str, image, template, method, mask=None) -> np.ndarray:
         mh, mw = mask.shape
         valid = (mh, mw) == (h, w) and W >= w and H >= h
         out = _lib.host_empty((H - h + 1, W - w + 1) if valid else (1, 1))
-        check(fn(_ptr(image, C.c_uint8), W, H, _ptr(template, C.c_uint8), w, h, int(m),
-                 _ptr(mask, C.c_uint8), mw, mh, _ptr(out, C.c_float)))
+        check(fn(_ptr(image), W, H, _ptr(template), w, h, int(m), _ptr(mask), mw, mh, _ptr(out)))
         return out
     valid = W >= w and H >= h
     out = _lib.host_empty((H - h + 1, W - w + 1) if valid else (1, 1))
-    check(fn(_ptr(image, C.c_uint8), W, H, _ptr(template, C.c_uint8), w, h, int(m),
-             _ptr(out, C.c_float)))
+    check(fn(_ptr(image), W, H, _ptr(template), w, h, int(m), _ptr(out)))
     return out
 
 
