@@ -475,7 +475,8 @@ def run_learned(args, world, rank, local) -> dict:
 
     n_scenes = args.learned_scenes
     seeds = [5 + rank * 1000 + k for k in range(n_scenes)]
-    with mp.get_context("spawn").Pool(min(n_scenes, os.cpu_count() or 1)) as pool:
+    procs = max(1, min(n_scenes, (os.cpu_count() or 1) // max(world, 1), 8))  # host RAM per rank
+    with mp.get_context("spawn").Pool(procs) as pool:
         scenes = pool.map(_learned_scene, seeds)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
@@ -794,6 +795,7 @@ def run_ours(args, world, rank, local):
     int8_peak_tops = 2.0 * pk["bf16_tflops"]
     dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["total_ms"]) if kernels else (None, None)
     roofline = None
+    notes = {}
     if dom:
         per_launch_s = dom["total_ms"] / dom["launches"] / 1e3
         macs_per_launch = dom["algorithmic_macs"] / dom["launches"]
@@ -802,15 +804,15 @@ def run_ours(args, world, rank, local):
         roofline = {"bound": "tensor", "achieved": achieved, "peak": int8_peak_tops,
                     "unit": "TOP/s", "frac": achieved / int8_peak_tops, "traffic": traffic,
                     "kernel": dom_name, "launch_ms": per_launch_s * 1e3,
-                    "peak_note": (f"int8 dense = 2 x bf16 dense {pk['bf16_tflops']} TFLOP/s "
-                                  f"({pk['source']}, MEASURED_PEAKS.json); achieved counts 2 ops "
-                                  "per algorithmic MAC"),
-                    "timing_note": ("the step's two launches (unmasked and binary-mask groups) run "
-                                    "side by side on two streams and are timed as one CUDA-event "
-                                    "span on the plan's stream; launch_ms = span / 2, achieved = "
-                                    "both launches' MACs / span"),
                     "hbm_frac": (dom["algorithmic_bytes"] / dom["launches"] / per_launch_s / 1e9)
                     / pk["hbm_gbs"]}
+        notes["roofline_peak"] = (f"int8 dense = 2 x bf16 dense {pk['bf16_tflops']} TFLOP/s "
+                                  f"({pk['source']}, MEASURED_PEAKS.json); achieved counts 2 ops "
+                                  "per algorithmic MAC")
+        notes["roofline_timing"] = ("the step's two launches (unmasked and binary-mask groups) run "
+                                    "side by side on two streams and are timed as one CUDA-event "
+                                    "span on the plan's stream; launch_ms = span / 2, achieved = "
+                                    "both launches' MACs / span")
         # the banded-Toeplitz formulation issues more MACs than the algorithmic
         # count: the pipe-level fraction counts the MACs the kernel executes
         ratios = {"unmasked": executed_mac_ratio(W_IMG, H_IMG, T, T, False),
@@ -818,8 +820,10 @@ def run_ours(args, world, rank, local):
         executed_per_step = MAC_PER_MAP * 4 * (ratios["unmasked"]["ratio"] + ratios["binary_mask"]["ratio"])
         roofline["executed_mac_ratio"] = {k: round(v["ratio"], 4) for k, v in ratios.items()}
         roofline["pipe_frac"] = roofline["frac"] * executed_per_step / MAC_PER_STEP
-        roofline["ceiling_note"] = ("with the tensor pipe saturated the step reaches at most "
-                                    f"{MAC_PER_STEP / executed_per_step:.3f} of the int8 peak in algorithmic MACs")
+        roofline["ceiling"] = MAC_PER_STEP / executed_per_step
+        notes["roofline_ceiling"] = ("ceiling: with the tensor pipe saturated the step reaches at most "
+                                     "that fraction of the int8 peak in algorithmic MACs; pipe_frac "
+                                     "counts the MACs the kernel executes")
     total_kernel_ms = sum(k["total_ms"] for k in kernels.values()) or 1.0
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -843,6 +847,7 @@ def run_ours(args, world, rank, local):
         "graph_ms_per_step": graph_ms / args.steps,
         "roofline": roofline,
         "cpu_baseline": cpu,
+        "summary": config_summary(learned, many, side),
         "learned": learned,
         "many_templates": many,
         **side,
@@ -858,9 +863,39 @@ def run_ours(args, world, rank, local):
         "fp64_oracle_error": ("0 ulp: all eight maps of this workload equal the FP64 oracle's bit for "
                               "bit (tests/test_gpu_parity.py::test_blob_scene_1920x1080_template_64_exact); "
                               "the reference arm's line reports the reference's own f32 error"),
+        "notes": notes,
         "next_rows": nxt,
     }
     print(json.dumps(line), flush=True)
+
+
+def config_summary(learned, many, side) -> dict:
+    """The other configurations' headline figures in a few hundred bytes, so
+    that a truncated view of the line still carries them (the full objects
+    follow)."""
+    r = lambda v, n=1: None if v is None else round(v, n)  # noqa: E731
+    out = {}
+    sm = side.get("small_map") if side else None
+    if sm:
+        out["config1_small_map"] = {"GMAC_s": r(sm["value"]), "us_per_map": r(sm["us_per_map"]),
+                                    "e2e_us_per_map": r(sm["e2e"]["us_per_map"])}
+    bu = side.get("batch_uneven") if side else None
+    if bu:
+        out["config3_batch"] = {"GMAC_s": r(bu["value"]), "ms_per_batch": r(bu["ms_per_batch"], 2),
+                                "kernels_per_batch": bu["kernels_per_batch"],
+                                "frac": r(bu["roofline"]["frac"], 3)}
+    if many:
+        out["config4_many"] = {"GMAC_s": r(many["value"]), "ms_per_query": r(many["ms_per_query"], 2),
+                               "hbm_frac": r(many["roofline"]["frac"], 3), "argmax_at_crop": many["argmax_at_crop"]}
+    if learned:
+        lc = learned.get("learned_certificate_only", {})
+        out["config5_learned"] = {
+            "exhaustive_q_s": r(learned["exhaustive"]["queries_per_s"]),
+            "learned_q_s": r(learned["learned"]["queries_per_s"]), "speedup": r(learned["speedup"], 2),
+            "agreement": learned["agreement"], "queries": learned["queries"],
+            "certificate_only_q_s": r(lc.get("queries_per_s")),
+            "certificate_only_agreement": lc.get("agreement")}
+    return out
 
 
 def main():

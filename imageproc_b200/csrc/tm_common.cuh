@@ -116,7 +116,7 @@ __device__ __forceinline__ float norm_quotient_fp64_w(uint32_t s, double w, uint
 }
 
 // The common case of norm_quotient_fp64_w without branches, for epilogues
-// that score many values independently: w > 0 is a normal double and s > 0.
+// that score many values independently: w > 0 is a normal double.
 // a = RN(s w) comes from one fused multiply-add, fma(2^52 + s, w, -2^52 w):
 // 2^52 + s is s's bits under the exponent of 2^52 (exact for s < 2^32),
 // -2^52 w is w with 52 added to its exponent and the sign set (one integer
@@ -124,17 +124,18 @@ __device__ __forceinline__ float norm_quotient_fp64_w(uint32_t s, double w, uint
 // double as RN(RN_d(s) * w). The midpoint window is 2^8 units of a's last
 // place on either side: a is fewer than 2^5 units from q (the bound of
 // norm_quotient_fp64_w), so a value outside the window rounds to the same
-// f32 as q. `undecided` is set
-// when the result must come from norm_quotient_fp64_w instead (s == 0, or
-// a inside the window).
+// f32 as q. `undecided` is set when the result must come from
+// norm_quotient_fp64_w instead (a inside the window). s == 0 gives a == 0, whose high word is clamped up to the bias
+// difference so that the formed bits are those of +0.0f, the zero-score rule.
 __device__ __forceinline__ uint32_t norm_bits_fp64_fast(uint32_t s, double w, bool& undecided) {
   const double d = __hiloint2double(0x43300000, (int)s);
   const double nc = __hiloint2double((int)((uint32_t)__double2hiint(w) + 0x83400000u), __double2loint(w));
   const double a = __fma_rn(d, w, nc);
   const uint32_t ahi = (uint32_t)__double2hiint(a), alo = (uint32_t)__double2loint(a);
   const uint32_t dropped = alo & 0x1FFFFFFFu;
-  undecided |= (dropped - (0x10000000u - 0x100u) < 0x200u) | (s == 0u);
-  return (((ahi - (896u << 20)) << 3) | (alo >> 29)) + (dropped >> 28);
+  undecided |= dropped - (0x10000000u - 0x100u) < 0x200u;
+  const uint32_t hi = max(ahi, 896u << 20);  // a == 0: every formed bit is zero
+  return (((hi - (896u << 20)) << 3) | (alo >> 29)) + (dropped >> 28);
 }
 
 // finish_score for callers whose X, Y and TSS are all below 2^31 (templates
