@@ -52,7 +52,7 @@ constexpr int kMaxTopK = 16;
 constexpr int kWin = 32;          // verification window: 32 x 32 positions
 constexpr int kBlk = 12;          // certification block: 12 x 12 positions
 constexpr int kMaxExtra = 16384;  // most extra 4 x 4 blocks a template may verify
-constexpr int kVerifySlices = 32;  // blocks of threads per template verifying extra blocks
+constexpr int kVerifyCtas = 4 * 148;  // blocks of threads sharing all templates' extra blocks
 constexpr uint32_t kFallbackPerTemplate = 8;  // fallbacks up to this many use the single-template kernel
 constexpr int kPatch = kWin + kTpl - 1;        // 79 image rows / columns per window
 constexpr int kPatchPitch = 96;                // 16-byte multiple >= kPatch + 4
@@ -663,56 +663,122 @@ __global__ void __launch_bounds__(256) certify_l3_kernel(const uint8_t* __restri
   }
 }
 
+// offsets[t] = sum of the verified block counts of templates < t (a count
+// above kMaxExtra counts 0: that template falls back), offsets[T] = total.
+// One block of 1024 threads; templates in chunks of 1024.
+__global__ void __launch_bounds__(1024) extra_offsets_kernel(const uint32_t* __restrict__ n_extra, uint32_t T,
+                                                             uint32_t* __restrict__ offsets) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < T; base += blockDim.x) {
+    const uint32_t t = base + threadIdx.x;
+    uint32_t v = 0;
+    if (t < T) {
+      v = n_extra[t];
+      v = v > (uint32_t)kMaxExtra ? 0u : v;
+    }
+    uint32_t incl = v;  // inclusive scan in the warp
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+      if ((int)lane >= d) incl += o;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < (blockDim.x >> 5) ? s_warp[lane] : 0u;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, w, d);
+        if ((int)lane >= d) w += o;
+      }
+      s_warp[lane] = w;  // inclusive warp totals
+    }
+    __syncthreads();
+    const uint32_t before = s_carry + (warp ? s_warp[warp - 1] : 0u) + incl - v;
+    if (t < T) offsets[t] = before;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) offsets[T] = s_carry;
+}
+
 // Exact minimum over the extra blocks of 4 x 4 positions (packed micro-block
-// indices py * Pmx + px from certify_kernel), every block of every template
-// whose list fits: grid (slices, template), one warp per block. The warp
-// stages the block's image patch (51 rows x 13 words; W is a multiple of 32
-// and 4 px is a multiple of 4, so the words are aligned; words past the
-// image read as zero, and feed no valid position) in its own shared memory,
-// then: R(r, ox) = sum of I^2 over 48 bytes of patch row r from column ox
-// (51 x 4 sums, dp4a), Y(ox, oy) = sum over 48 rows of R; X by lanes = 16
-// positions x 2 halves of the template's rows, dp4a on byte_perm-shifted
-// patch words; the halves meet through one shuffle and SSE = Y - 2X + TSS
-// rounds once to f32 as in verify_kernel. The first minimum goes to best[t].
+// indices py * Pmx + px from certify_kernel) of every template whose list
+// fits. All templates' blocks form one sequence (offsets from
+// extra_offsets_kernel) that the grid's warps share in contiguous slices, so
+// a template with many blocks is spread over the whole GPU. Per block, one
+// warp stages the block's image patch (51 rows x 13 words; W is a multiple of
+// 32 and 4 px a multiple of 4, so the words are aligned; words past the image
+// read as zero and feed no valid position) in its own shared memory, then:
+// R(r, ox) = sum of I^2 over 48 bytes of patch row r from column ox (51 x 4
+// sums, dp4a), Y(ox, oy) = sum over 48 rows of R; X by lanes = 16 positions x
+// 2 halves of the template's rows, dp4a on byte_perm-shifted patch words
+// against the template staged in the warp's shared memory when the slice
+// reaches a new template; the halves meet through one shuffle and SSE =
+// Y - 2X + TSS rounds once to f32 as in verify_kernel. Each warp folds its
+// first minimum per template into best[t].
 constexpr int kPatchRows = 4 + kTpl - 1;        // 51
 constexpr int kPatchWords = (4 + kTpl + 3) / 4;  // 13 (52 bytes >= 51)
-__global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
-                                                            const uint8_t* __restrict__ tpl,
-                                                            const uint32_t* __restrict__ extra,
-                                                            const uint32_t* __restrict__ n_extra, uint32_t Pmx,
-                                                            uint32_t Wo, uint32_t Ho,
-                                                            unsigned long long* __restrict__ best) {
-  __shared__ uint32_t s_tpl[kTpl][kTpl / 4 + 1];  // padded: the two row halves fall in different banks
-  __shared__ uint32_t s_patch[8][kPatchRows][kPatchWords];
-  __shared__ uint32_t s_rsq[8][kPatchRows][4];
-  __shared__ unsigned long long s_tss[8];
-  __shared__ unsigned long long s_best[8];
-  const uint32_t t = blockIdx.y;
-  const uint32_t n = n_extra[t];
-  if (n == 0 || n > (uint32_t)kMaxExtra) return;  // nothing listed, or the template falls back
-  const uint32_t* tw = reinterpret_cast<const uint32_t*>(tpl + (size_t)t * kTpl * kTpl);
-  unsigned long long tss = 0ull;
-  for (uint32_t i = threadIdx.x; i < (uint32_t)(kTpl * kTpl / 4); i += blockDim.x) {
-    const uint32_t v = tw[i];
-    s_tpl[i / (kTpl / 4)][i % (kTpl / 4)] = v;
-    tss += __dp4a(v, v, 0u);
-  }
-  for (int d = 16; d; d >>= 1) tss += __shfl_xor_sync(0xffffffffu, tss, d);
+constexpr int kVerifyWarps = 8;
+__global__ void __launch_bounds__(kVerifyWarps * 32) verify_blocks_kernel(
+    const uint8_t* __restrict__ img, uint32_t W, uint32_t H, const uint8_t* __restrict__ tpl,
+    const uint32_t* __restrict__ extra, const uint32_t* __restrict__ offsets, uint32_t T, uint32_t Pmx,
+    uint32_t Wo, uint32_t Ho, unsigned long long* __restrict__ best) {
+  __shared__ uint32_t s_tpl[kVerifyWarps][kTpl][kTpl / 4 + 1];  // padded: the two row halves in different banks
+  __shared__ uint32_t s_patch[kVerifyWarps][kPatchRows][kPatchWords];
+  __shared__ uint32_t s_rsq[kVerifyWarps][kPatchRows][4];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) s_tss[warp] = tss;
-  __syncthreads();
-  tss = 0ull;
-  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tss += s_tss[k];
+  const uint32_t total = offsets[T];
+  const uint32_t nwarps = gridDim.x * kVerifyWarps, gw = blockIdx.x * kVerifyWarps + warp;
+  const uint32_t chunk = (total + nwarps - 1) / nwarps;
+  const uint32_t beg = min(total, gw * chunk), end = min(total, beg + chunk);
+  if (beg >= end) return;
   const uint32_t pos = lane & 15u, half = lane >> 4;
   const uint32_t ox = pos & 3u, oy = pos >> 2;
   const uint32_t sel = 0x3210u + ox * 0x1111u;
-  unsigned long long mykey = ~0ull;
   const uint32_t* const img32 = reinterpret_cast<const uint32_t*>(img);
   const uint32_t wpr = W / 4;  // words per image row
+  uint32_t (*tw)[kTpl / 4 + 1] = s_tpl[warp];
   uint32_t (*patch)[kPatchWords] = s_patch[warp];
   uint32_t (*rsq)[4] = s_rsq[warp];
-  for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + warp; i < n; i += gridDim.x * (blockDim.x >> 5)) {
-    const uint32_t mb = extra[(size_t)t * kMaxExtra + i];
+  // the template of the slice's first block: offsets[t] <= beg < offsets[t + 1]
+  uint32_t lo = 0, hi = T;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (offsets[mid] <= beg) lo = mid;
+    else hi = mid;
+  }
+  uint32_t t = lo, t_end = offsets[t + 1];
+  while (t_end <= beg) t_end = offsets[++t + 1];  // skip templates with no blocks
+  bool staged = false;
+  unsigned long long tss = 0ull, mykey = ~0ull;
+  for (uint32_t i = beg; i < end; ++i) {
+    if (i >= t_end || !staged) {
+      if (staged) {  // the slice moves to the next template: fold this one's minimum
+        for (int d = 16; d; d >>= 1) {
+          const unsigned long long o = __shfl_xor_sync(0xffffffffu, mykey, d);
+          mykey = o < mykey ? o : mykey;
+        }
+        if (lane == 0 && mykey != ~0ull) atomicMin(best + t, mykey);
+        mykey = ~0ull;
+        while (t_end <= i) t_end = offsets[++t + 1];
+      }
+      __syncwarp();  // the previous template's words are no longer read
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(tpl + (size_t)t * kTpl * kTpl);
+      uint32_t part = 0;
+      for (uint32_t e = lane; e < (uint32_t)(kTpl * kTpl / 4); e += 32) {
+        const uint32_t v = __ldg(src + e);
+        tw[e / (kTpl / 4)][e % (kTpl / 4)] = v;
+        part = __dp4a(v, v, part);
+      }
+      for (int d = 16; d; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
+      tss = part;  // at most 2304 * 65025 < 2^32
+      staged = true;
+    }
+    const uint32_t mb = extra[(size_t)t * kMaxExtra + (i - offsets[t])];
     const uint32_t x0 = 4 * (mb % Pmx), y0 = 4 * (mb / Pmx);
     __syncwarp();  // the previous block's reads of the patch are done
     for (uint32_t e = lane; e < (uint32_t)(kPatchRows * kPatchWords); e += 32) {
@@ -743,7 +809,7 @@ __global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __res
 #pragma unroll
       for (int k = 0; k < kTpl / 4; ++k) {
         const uint32_t nxt = prow[k + 1];
-        X = __dp4a(__byte_perm(cur, nxt, sel), s_tpl[dy][k], X);
+        X = __dp4a(__byte_perm(cur, nxt, sel), tw[dy][k], X);
         cur = nxt;
       }
     }
@@ -764,13 +830,7 @@ __global__ void __launch_bounds__(256) verify_blocks_kernel(const uint8_t* __res
     const unsigned long long o = __shfl_xor_sync(0xffffffffu, mykey, d);
     mykey = o < mykey ? o : mykey;
   }
-  if (lane == 0) s_best[warp] = mykey;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long b = s_best[0];
-    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) b = s_best[k] < b ? s_best[k] : b;
-    if (b != ~0ull) atomicMin(best + t, b);
-  }
+  if (lane == 0 && mykey != ~0ull) atomicMin(best + t, mykey);
 }
 
 // Windows of caller-given proposals: template origins (y * Wo + x, k per
@@ -870,6 +930,7 @@ struct Carve {
   uint32_t* list1;  // certification work lists: per template cap1 64 x 64 blocks,
   uint32_t* list2;  // kMaxLevel2 16 x 16 blocks,
   uint32_t* n12;    // and their counts (n1: T words, then n2: T words)
+  uint32_t* offsets;  // T + 1 prefix offsets of the verified extra blocks
   uint32_t cap1;
   unsigned long long* best;
   uint32_t* micro;
@@ -913,6 +974,7 @@ Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
   c.list1 = reinterpret_cast<uint32_t*>(take((size_t)T * c.cap1 * 4));
   c.list2 = reinterpret_cast<uint32_t*>(take((size_t)T * kMaxLevel2 * 4));
   c.n12 = reinterpret_cast<uint32_t*>(take((size_t)T * 8));
+  c.offsets = reinterpret_cast<uint32_t*>(take((size_t)(T + 1) * 4));
   c.best = reinterpret_cast<unsigned long long*>(take((size_t)T * 8));
   const uint32_t Mx = (W - kBlk + 1 + 3) / 4, My = (H - kBlk + 1 + 3) / 4;
   c.micro = reinterpret_cast<uint32_t*>(take((size_t)Mx * My * 4));
@@ -1015,7 +1077,9 @@ ipb_status finish_queries(ProposeScratch& ps, const Carve& c, unsigned int call_
                                                                Mx, My, Pmx, Pmy, Wo, Ho, c.list2, c.n12 + T, c.wins,
                                                                c.nwin, opt.top_k, c.extra, c.n_extra);
     count_launch(kKernelPropose);
-    verify_blocks_kernel<<<dim3(kVerifySlices, T), 256, 0, s>>>(d_image, W, H, d_templates, c.extra, c.n_extra,
+    extra_offsets_kernel<<<1, 1024, 0, s>>>(c.n_extra, T, c.offsets);
+    count_launch(kKernelPropose);
+    verify_blocks_kernel<<<kVerifyCtas, kVerifyWarps * 32, 0, s>>>(d_image, W, H, d_templates, c.extra, c.offsets, T,
                                                                    (Wo + 3) / 4, Wo, Ho, c.best);
     count_launch(kKernelPropose);
     P_CUDA(cudaGetLastError(), "certification");

@@ -93,7 +93,7 @@ def _gray(img: np.ndarray, what: str) -> np.ndarray:
 
 
 def _ptr(a: np.ndarray):
-    return a.ctypes.data if a.size else None
+    return a.ctypes.data  # numpy gives empty arrays an address too
 
 
 def _run(fn_name: str, image, template, method, mask=None) -> np.ndarray:
