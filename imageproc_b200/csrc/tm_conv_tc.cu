@@ -91,6 +91,7 @@ struct TcArgs {
   uint32_t stall;       // pipeline_stall() at launch
   unsigned int* err;    // error word or null
   unsigned int tag;
+  const uint4* mask;    // or null: keeps an output bf16 only where this activation is > 0 (ReLU')
 };
 
 __global__ void __launch_bounds__(kThreadsTc) conv_tc_kernel(const TcArgs a) {
@@ -234,6 +235,16 @@ __global__ void __launch_bounds__(kThreadsTc) conv_tc_kernel(const TcArgs a) {
             }
             pk[e] = (uint32_t)bf16_rn(lo) | ((uint32_t)bf16_rn(hi) << 16);
           }
+          if (a.mask) {
+            // the data gradient: times ReLU'(Z) = [A > 0] of the layer's activation
+            const uint4 mk = a.mask[(((size_t)n * a.H + y) * kChunks + c) * a.W + x];
+            const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const bool plo = (int16_t)(mw[e] & 0xFFFFu) > 0, phi = (int16_t)(mw[e] >> 16) > 0;
+              pk[e] &= (plo ? 0x0000FFFFu : 0u) | (phi ? 0xFFFF0000u : 0u);
+            }
+          }
           dst[(size_t)c * a.W] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
       }
@@ -257,7 +268,7 @@ __global__ void __launch_bounds__(kThreadsTc) conv_tc_kernel(const TcArgs a) {
 
 cudaError_t launch_conv_tc(const uint4* in, uint32_t n, uint32_t H, uint32_t W, const uint16_t* wt,
                            const float* bias, int relu, uint4* out, unsigned int* err, unsigned int tag,
-                           cudaStream_t s) {
+                           cudaStream_t s, const uint4* mask) {
   if (n == 0 || H == 0 || W == 0) return cudaSuccess;
   static PerDeviceOnce attr;
   cudaError_t e = attr.run([] {
@@ -274,7 +285,7 @@ cudaError_t launch_conv_tc(const uint4* in, uint32_t n, uint32_t H, uint32_t W, 
   if (band < 4) band = 4;
   if (band > H) band = H;
   const dim3 grid(segs, (H + band - 1) / band, n);
-  TcArgs args{in, out, wt, bias, relu, H, W, band, pipeline_wait_ns(), pipeline_stall() ? 1u : 0u, err, tag};
+  TcArgs args{in, out, wt, bias, relu, H, W, band, pipeline_wait_ns(), pipeline_stall() ? 1u : 0u, err, tag, mask};
   conv_tc_kernel<<<grid, kThreadsTc, TcSmemLayout::total, s>>>(args);
   count_launch(kKernelLearned);
   return cudaGetLastError();

@@ -7,6 +7,7 @@
 // embedding head of training, the softmax loss and Adam run on CUDA cores.
 // Backward passes treat the bf16 roundings of the forward pass as the identity.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -706,11 +707,23 @@ struct ipb_proposal_net {
   // training scratch (grow-only)
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // error word of the tcgen05 convolutions of training steps (after the
+  // parameters in the same allocation) and the tag of the last step
+  unsigned int* err = nullptr;
+  unsigned int tag = 0;
 };
 
 namespace ipb {
 namespace learned {
 const PackedWeights& net_weights(const ipb_proposal_net* net) { return net->pw; }
+
+bool learned_use_mma() {
+  static const bool v = [] {
+    const char* e = std::getenv("IPB_LEARNED_KERNELS");
+    return e && std::strcmp(e, "mma") == 0;
+  }();
+  return v;
+}
 }  // namespace learned
 }  // namespace ipb
 
@@ -778,7 +791,7 @@ TrainCarve carve(uint8_t* base, uint32_t N, uint32_t sh, uint32_t sw, uint32_t T
 
 // backward through the trunk of one side (scenes or templates): dz5 in d0
 ipb_status trunk_backward(ipb_proposal_net* net, const uint8_t* img, uint32_t n, uint32_t h, uint32_t w,
-                          uint4* const* acts, uint4* d0, uint4* d1, cudaStream_t s) {
+                          uint4* const* acts, uint4* d0, uint4* d1, cudaStream_t s, bool tc) {
   const uint32_t H = h / 4, W = w / 4;
   uint4* dz = d0;
   uint4* other = d1;
@@ -789,8 +802,9 @@ ipb_status trunk_backward(ipb_proposal_net* net, const uint8_t* img, uint32_t n,
     count_launch(kKernelLearned);
     NET_CUDA(cudaGetLastError(), "weight gradient");
     // data gradient into A_l, times relu'(Z_l) = [A_l > 0]
-    NET_CUDA(launch_conv_mma(dz, n, H, W, net->pw.bwd + (size_t)(l - 1) * 9 * kC * kC, nullptr, 0, acts[l - 1],
-                             other, s),
+    const uint16_t* wb = net->pw.bwd + (size_t)(l - 1) * 9 * kC * kC;
+    NET_CUDA(tc ? launch_conv_tc(dz, n, H, W, wb, nullptr, 0, other, net->err, net->tag, s, acts[l - 1])
+                : launch_conv_mma(dz, n, H, W, wb, nullptr, 0, acts[l - 1], other, s),
              "data gradient");
     std::swap(dz, other);
   }
@@ -824,8 +838,16 @@ ipb_status loss_and_grads(ipb_proposal_net* net, const uint8_t* scenes, uint32_t
   NET_CUDA(cudaMemsetAsync(c.loss, 0, sizeof(float), s), "memset");
   NET_CUDA(cudaMemsetAsync(c.dG, 0, sizeof(float) * T * kEmb, s), "memset");
   NET_CUDA(launch_pack_weights(net->params, net->pw, s), "pack weights");
-  NET_CUDA(launch_trunk(scenes, N, sh, sw, net->pw, c.acts_s, nullptr, nullptr, c.Fs, s), "scene trunk");
-  NET_CUDA(launch_trunk(templates, T, kTpl, kTpl, net->pw, c.acts_t, nullptr, nullptr, c.Ft, s), "template trunk");
+  // the 32-channel convolutions and their data gradients on tcgen05 (or
+  // mma.sync with IPB_LEARNED_KERNELS=mma); the weight gradients on mma.sync
+  const bool tc = !learned_use_mma();
+  const int kernel = tc ? 0 : 1;
+  net->tag += 1;
+  NET_CUDA(launch_trunk(scenes, N, sh, sw, net->pw, c.acts_s, nullptr, nullptr, c.Fs, s, kernel, net->err, net->tag),
+           "scene trunk");
+  NET_CUDA(launch_trunk(templates, T, kTpl, kTpl, net->pw, c.acts_t, nullptr, nullptr, c.Ft, s, kernel, net->err,
+                        net->tag),
+           "template trunk");
   NET_CUDA(launch_embed(c.Ft, T, c.G, s), "embedding");
   const size_t head_smem = sizeof(float) * (kHeadPos * (kEmb + 1) + T * kEmb);
   const unsigned nblk = (unsigned)((P + kHeadPos - 1) / kHeadPos);
@@ -856,13 +878,17 @@ ipb_status loss_and_grads(ipb_proposal_net* net, const uint8_t* scenes, uint32_t
   embed_grad_kernel<<<(tu + 255) / 256, 256, 0, s>>>(c.dG, T, c.dt_a);
   count_launch(kKernelLearned);
   NET_CUDA(cudaGetLastError(), "embedding gradient");
-  ipb_status st = trunk_backward(net, scenes, N, sh, sw, c.acts_s, c.d_a, c.d_b, s);
+  ipb_status st = trunk_backward(net, scenes, N, sh, sw, c.acts_s, c.d_a, c.d_b, s, tc);
   if (st != IPB_OK) return st;
-  st = trunk_backward(net, templates, T, kTpl, kTpl, c.acts_t, c.dt_a, c.dt_b, s);
+  st = trunk_backward(net, templates, T, kTpl, kTpl, c.acts_t, c.dt_a, c.dt_b, s, tc);
   if (st != IPB_OK) return st;
   if (h_loss) {
+    unsigned int failed = 0;
     NET_CUDA(cudaMemcpyAsync(h_loss, c.loss, sizeof(float), cudaMemcpyDeviceToHost, s), "copy loss");
+    NET_CUDA(cudaMemcpyAsync(&failed, net->err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s), "copy error word");
     NET_CUDA(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (failed >= net->tag && failed != 0)
+      return net_fail(IPB_ERR_TIMEOUT, "a training convolution timed out waiting on its pipeline");
   }
   return IPB_OK;
 }
@@ -878,7 +904,7 @@ IPB_API ipb_status ipb_proposal_net_create(const float* params, ipb_proposal_net
   if (major != 10) return net_fail(IPB_ERR_NO_DEVICE, "imageproc_b200 needs an sm_100 (B200) device");
   auto* net = new ipb_proposal_net();
   net->device = dev;
-  cudaError_t e = cudaMalloc(&net->params, sizeof(float) * kParams * 4);
+  cudaError_t e = cudaMalloc(&net->params, sizeof(float) * kParams * 4 + 16);
   if (e == cudaSuccess) e = cudaMalloc(&net->pw_block, kPwBytes);
   if (e != cudaSuccess) {
     if (net->params) cudaFree(net->params);
@@ -888,13 +914,14 @@ IPB_API ipb_status ipb_proposal_net_create(const float* params, ipb_proposal_net
   net->grads = net->params + kParams;
   net->adam_m = net->params + 2 * kParams;
   net->adam_v = net->params + 3 * kParams;
+  net->err = reinterpret_cast<unsigned int*>(net->params + 4 * kParams);
   uint8_t* pb = static_cast<uint8_t*>(net->pw_block);
   net->pw.fwd = reinterpret_cast<uint16_t*>(pb);
   net->pw.bwd = net->pw.fwd + 4 * 9 * kC * kC;
   net->pw.w1 = reinterpret_cast<float*>(net->pw.bwd + 4 * 9 * kC * kC);
   net->pw.bias = net->pw.w1 + kC * 9;
   e = cudaMemcpy(net->params, params, sizeof(float) * kParams, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(net->adam_m, 0, sizeof(float) * 2 * kParams);
+  if (e == cudaSuccess) e = cudaMemset(net->adam_m, 0, sizeof(float) * 2 * kParams + 16);
   if (e == cudaSuccess) e = launch_pack_weights(net->params, net->pw, nullptr);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {

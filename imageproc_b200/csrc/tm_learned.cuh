@@ -62,11 +62,16 @@ cudaError_t launch_conv1(const uint8_t* img, uint32_t n, uint32_t h, uint32_t w,
 cudaError_t launch_conv_mma(const uint4* in, uint32_t n, uint32_t H, uint32_t W, const uint16_t* wt,
                             const float* bias, int relu, const uint4* mask, uint4* out, cudaStream_t s);
 // the same convolution on tcgen05 (kind::f16, accumulators in tensor memory):
-// out = bf16(act(bias + conv(wt, in))); a bounded wait that runs out stores
+// out = bf16(act(bias + conv(wt, in))), times [mask > 0] when mask is not null
+// (the data gradient of a ReLU layer); a bounded wait that runs out stores
 // `tag` into *err (when err is not null)
 cudaError_t launch_conv_tc(const uint4* in, uint32_t n, uint32_t H, uint32_t W, const uint16_t* wt,
                            const float* bias, int relu, uint4* out, unsigned int* err, unsigned int tag,
-                           cudaStream_t s);
+                           cudaStream_t s, const uint4* mask = nullptr);
+// IPB_LEARNED_KERNELS=mma: the network's 32-channel convolutions and heatmap
+// on the mma.sync kernels instead of tcgen05 (same arithmetic: bf16 operands,
+// fp32 accumulation), in queries and in training; for testing and measurement.
+bool learned_use_mma();
 // the trunk: conv1 + four tensor-core layers; acts (4 buffers) keeps A1..A4
 // when not null (training), otherwise ping-pong buffers a/b are used.
 // kernel: 0 = tcgen05 (launch_conv_tc), 1 = mma.sync (launch_conv_mma)

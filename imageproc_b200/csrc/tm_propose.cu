@@ -987,16 +987,7 @@ Carve carve(uint8_t* base, uint32_t W, uint32_t H, uint32_t T, uint32_t k) {
   return c;
 }
 
-// IPB_LEARNED_KERNELS=mma runs the query's convolutions and heatmap on the
-// mma.sync kernels of the training path instead of tcgen05 (same arithmetic:
-// bf16 operands, fp32 accumulation); for testing and measurement.
-bool use_mma_kernels() {
-  static const bool v = [] {
-    const char* e = std::getenv("IPB_LEARNED_KERNELS");
-    return e && std::strcmp(e, "mma") == 0;
-  }();
-  return v;
-}
+bool use_mma_kernels() { return learned_use_mma(); }
 
 ProposeScratch& scratch_for_thread() {
   thread_local ProposeScratch s;

@@ -172,12 +172,6 @@ __device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t
   return rs;
 }
 
-// Order-preserving key of a finite f32 score (larger value -> larger key).
-__device__ __forceinline__ uint32_t order_key(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
 // A builder warp's share of a tile's epilogue: columns [c_begin, c_begin +
 // ncols) of the accumulators for its 32 lanes (output columns).
 struct UmmaEpi {
@@ -187,33 +181,36 @@ struct UmmaEpi {
   uint32_t Y;            // unmasked: window sum of the first column (row c_begin)
 };
 
-// Scores with the method and precision fixed at compile time, so the 16
-// scores of each tensor-memory load are straight-line code.
+// Scores with the method and precision fixed at compile time, so the
+// kEpiCols scores of each tensor-memory load are straight-line code (eight:
+// the accumulator, Y and its two sliding inputs stay within the registers
+// the 544-thread block leaves each thread).
+constexpr int kEpiCols = 8;
 template <bool MASKED, int kMethod, int kPrec, bool kExt>
 __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
   const UmmaProblem& q = *e.q;
   uint32_t Y = e.Y;
   unsigned long long kmin = ~0ull, kmax = 0ull;
-  for (uint32_t n0 = e.c_begin; n0 < e.c_begin + e.ncols; n0 += 16) {
-    uint32_t vx[16];
-    tmem_ld16(tmem_addr(e.tmem, e.lane_base, n0), vx);
-    uint32_t yv[16];
+  for (uint32_t n0 = e.c_begin; n0 < e.c_begin + e.ncols; n0 += kEpiCols) {
+    uint32_t vx[kEpiCols];
+    tmem_ld8(tmem_addr(e.tmem, e.lane_base, n0), vx);
+    uint32_t yv[kEpiCols];
     if constexpr (MASKED && kMethod == kCcorr) {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) yv[k] = 0u;  // not computed: CrossCorrelation is X alone
+      for (int k = 0; k < kEpiCols; ++k) yv[k] = 0u;  // not computed: CrossCorrelation is X alone
     } else if constexpr (MASKED) {
-      tmem_ld16(tmem_addr(e.tmem, e.lane_base, e.NT + n0), yv);
+      tmem_ld8(tmem_addr(e.tmem, e.lane_base, e.NT + n0), yv);
     } else {
       // window sums of the chunk: loads first, then the sliding chain
-      uint32_t add[16], subv[16];
+      uint32_t add[kEpiCols], subv[kEpiCols];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kEpiCols; ++k) {
         const uint32_t ra = n0 + k + q.h, rb = n0 + k;
         add[k] = ra < e.nrows ? e.s_rs[ra * kM + e.m] : 0u;
         subv[k] = rb < e.nrows ? e.s_rs[rb * kM + e.m] : 0u;
       }
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kEpiCols; ++k) {
         yv[k] = Y;
         Y += add[k];
         Y -= subv[k];
@@ -221,14 +218,14 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
     }
     tmem_wait_ld();
     // scores are never negative, so their f32 bits order like the values;
-    // the lane's 16 positions are rows of one column in index order, so the
-    // strict comparisons keep each extreme's first occurrence in the batch
+    // the lane's positions are rows of one column in index order, so the
+    // strict comparisons keep each extreme's first occurrence in the chunk
     const uint32_t y_first = e.y0 + n0;
-    const int nv = e.x < q.Wo ? (y_first < q.Ho ? (int)min(16u, q.Ho - y_first) : 0) : 0;
+    const int nv = e.x < q.Wo ? (y_first < q.Ho ? (int)min((uint32_t)kEpiCols, q.Ho - y_first) : 0) : 0;
     uint32_t mn = 0xFFFFFFFFu, jmn = 0, mx = 0u, jmx = 0;
     float* orow = q.out ? q.out + (size_t)y_first * q.Wo + e.x : nullptr;  // null: extremes only
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
+    for (int k = 0; k < kEpiCols; ++k) {
       const uint32_t bk = __float_as_uint(finish_score32(kMethod, kPrec, vx[k], yv[k], e.tss));
       if (k < nv) {
         if (orow) orow[(size_t)k * q.Wo] = __uint_as_float(bk);
