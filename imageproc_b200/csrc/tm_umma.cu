@@ -7,10 +7,11 @@
 // (image, template) pairs of uneven sizes in one persistent launch, with
 // find_extremes (:479-511) optionally fused into the epilogue.
 //
-// Formulation. A CTA owns a tile of 128 output columns (x0 + m, m = tensor-
-// memory lane) by NT output rows (y0 + n, n = tensor-memory column). For each
-// image row r of the tile (r = 0 .. NT + h - 2, image row y0 + r) and each
-// correlation c, into accumulator a(c):
+// Formulation. A CTA owns a tile of 128 output columns (x0 + c(m) for
+// tensor-memory lane m, c = lane_column below, a permutation of 0..127) by NT
+// output rows (y0 + n, n = tensor-memory column). For each image row r of the
+// tile (r = 0 .. NT + h - 2, image row y0 + r) and each correlation c, into
+// accumulator a(c) (writing x0 + m for x0 + c(m)):
 //   A_r[m][k] = P_c[y0 + r][x0 + m + k]          (a Hankel row per lane)
 //   B_r[n][k] = Q_c[r - n][k]                     (0 <= r - n < h, else 0)
 //   D_a(c)[m][n] += sum_k A_r[m][k] * B_r[n][k]
@@ -33,8 +34,9 @@
 // -16 bytes. Only the 16-aligned band of n where B_r is non-zero is issued.
 //
 // A_r goes straight into tensor memory: sixteen builder warps (four per
-// tensor-memory lane quadrant) form each lane's K bytes from the staged image
-// rows with byte_perm and store them with tcgen05.st; the MMA reads A from
+// tensor-memory lane quadrant) read each lane's window of the staged image row
+// as aligned 16-byte chunks, form its K bytes with byte_perm and store them
+// with tcgen05.st; the MMA reads A from
 // tensor memory and only B from shared memory. Unmasked, the same words give
 // the lane's row sum of squares with dp4a, from which the epilogue slides the
 // window sum Y = sum I^2 over h rows, so no integral image is needed. The
@@ -132,25 +134,45 @@ __device__ void issue_tile_load(const UmmaLaunch& L, const UmmaProblem q, uint8_
   cp_async_commit();
 }
 
-// Builds one A row (one plane) for lane m into tensor memory; returns the
-// lane's row sum of squares over the template width when kRowSums.
-template <int KS, bool kRowSums>
-__device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t m, uint32_t w,
+// Output column (offset in the tile) of tensor-memory lane m = 32 q + l:
+// 16 (l / 4) + 4 q + (l % 4). Each lane quadrant q takes the columns whose
+// word offset within their 16-byte chunk is q, so a builder warp reads its
+// lanes' windows with aligned 16-byte loads and one compile-time word
+// offset; the four quadrants cover the tile's 128 columns once.
+__device__ __forceinline__ uint32_t lane_column(uint32_t m) {
+  return 16u * ((m & 31u) >> 2) + 4u * (m >> 5) + (m & 3u);
+}
+
+// Builds one A row (one plane) for lane l of lane quadrant Q into tensor
+// memory: the lane's window starts at byte 16 (l / 4) + 4 Q + (l % 4) of the
+// staged row, read as 16-byte chunks from chunk l / 4 on (the last byte read
+// is 128 + 4 KS, inside the row pitch). Returns the lane's row sum of
+// squares over the template width when kRowSums.
+template <int KS, bool kRowSums, int Q>
+__device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t l, uint32_t w,
                                               uint32_t taddr) {
-  const uint32_t* wp = reinterpret_cast<const uint32_t*>(plane_row) + (m >> 2);
-  const uint32_t sel = 0x3210u + (m & 3u) * 0x1111u;
+  const uint4* cp = reinterpret_cast<const uint4*>(plane_row) + (l >> 2);
+  const uint32_t sel = 0x3210u + (l & 3u) * 0x1111u;
   uint32_t rs = 0;
-  constexpr int CH = KS < 16 ? KS : 16;
+  // words per tensor-memory store: 16 for rows of 16 words; 8 otherwise, which
+  // keeps the wider rows within the 96 registers a thread has
+  constexpr int CH = KS == 16 ? 16 : 8;
   const uint32_t wq = w >> 2;
   const uint32_t tail = (w & 3u) ? ((1u << (8u * (w & 3u))) - 1u) : 0u;
-#pragma unroll
+  uint4 cur = cp[0];
+  // the 64-word rows run their eight groups as a loop (registers)
+#pragma unroll(KS == 64 ? 1 : KS / CH)
   for (int c0 = 0; c0 < KS; c0 += CH) {
-    uint32_t wv[CH + 1];
-#pragma unroll
-    for (int k = 0; k <= CH; ++k) wv[k] = wp[c0 + k];
+    // four words of A per chunk, from the chunk and the next one
     uint32_t a[CH];
 #pragma unroll
-    for (int k = 0; k < CH; ++k) a[k] = __byte_perm(wv[k], wv[k + 1], sel);
+    for (int j = 0; j < CH / 4; ++j) {
+      const uint4 nxt = cp[c0 / 4 + j + 1];
+      const uint32_t w8[8] = {cur.x, cur.y, cur.z, cur.w, nxt.x, nxt.y, nxt.z, nxt.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[4 * j + i] = __byte_perm(w8[Q + i], w8[Q + i + 1], sel);
+      cur = nxt;
+    }
     if constexpr (kRowSums) {
       if (c0 + CH <= (int)wq) {
         uint32_t r4[4] = {0u, 0u, 0u, 0u};
@@ -170,6 +192,34 @@ __device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t
     else tmem_st8(taddr + c0, a);
   }
   return rs;
+}
+
+// One builder warp's rows of a pipeline stage: rows r_first, r_first +
+// kSubs, ... below r_end, each row's planes into its tensor-memory columns;
+// unmasked, the lanes' row sums of squares go to s_rs[r][m].
+struct StageRows {
+  const uint8_t* img_buf;
+  uint32_t r_first, r_end, r0, tcol0, a_row_cols, imgp, plane_bytes, lane, m, w, tmem;
+  uint32_t* s_rs;
+  bool need_y;
+};
+
+template <int KS, bool MASKED, int Q>
+__device__ __forceinline__ void build_stage_rows(const StageRows& sr) {
+  constexpr int NPL = MASKED ? 3 : 1;
+  for (uint32_t r = sr.r_first; r < sr.r_end; r += kSubs) {
+    const uint32_t ta = tmem_addr(sr.tmem, Q * 32, sr.tcol0 + (r - sr.r0) * sr.a_row_cols);
+    const uint8_t* row = sr.img_buf + r * sr.imgp;
+    if constexpr (MASKED) {
+      build_row<KS, false, Q>(row, sr.lane, sr.w, ta);
+      if (sr.need_y) {
+#pragma unroll
+        for (int pl = 1; pl < NPL; ++pl) build_row<KS, false, Q>(row + pl * sr.plane_bytes, sr.lane, sr.w, ta + pl * KS);
+      }
+    } else {
+      sr.s_rs[r * kM + sr.m] = build_row<KS, true, Q>(row, sr.lane, sr.w, ta);
+    }
+  }
 }
 
 // A builder warp's share of a tile's epilogue: columns [c_begin, c_begin +
@@ -492,20 +542,16 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         }
         tc_fence_after();
         const uint32_t r0 = st * L.rps, r_end = min(nrows, r0 + L.rps);
-        // rows r == sub (mod kSubs) of this stage
-        for (uint32_t r = r0 + ((sub + kSubs - (r0 % kSubs)) % kSubs); r < r_end; r += kSubs) {
-          const uint32_t tcol = a_col0 + (s * L.rps + (r - r0)) * a_row_cols;
-          const uint8_t* row = img_buf + r * L.imgp;
-          if constexpr (MASKED) {
-            build_row<KS, false>(row, m, q.w, tmem_addr(tmem, lane_base, tcol));
-            if (need_y) {
-#pragma unroll
-              for (int pl = 1; pl < NPL; ++pl)
-                build_row<KS, false>(row + pl * L.plane_bytes, m, q.w, tmem_addr(tmem, lane_base, tcol + pl * KS));
-            }
-          } else {
-            s_rs[r * kM + m] = build_row<KS, true>(row, m, q.w, tmem_addr(tmem, lane_base, tcol));
-          }
+        // rows r == sub (mod kSubs) of this stage; the quadrant picks the
+        // compile-time word offset of the lanes' windows (warp-uniform)
+        const StageRows sr{img_buf, r0 + ((sub + kSubs - (r0 % kSubs)) % kSubs), r_end, r0,
+                           a_col0 + s * L.rps * a_row_cols, a_row_cols, L.imgp, L.plane_bytes,
+                           (uint32_t)lane, m, q.w, tmem, s_rs, need_y};
+        switch (q4) {
+          case 0: build_stage_rows<KS, MASKED, 0>(sr); break;
+          case 1: build_stage_rows<KS, MASKED, 1>(sr); break;
+          case 2: build_stage_rows<KS, MASKED, 2>(sr); break;
+          default: build_stage_rows<KS, MASKED, 3>(sr); break;
         }
         tmem_wait_st();
         tc_fence_before();
@@ -518,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       asm volatile("bar.sync 1, %0;" ::"n"(kBuilders) : "memory");
       if (ok) {
         tc_fence_after();
-        const uint32_t x = x0 + m;
+        const uint32_t x = x0 + lane_column(m);
         uint32_t Y = 0;  // window sums stay below 2^31 on this path
         if constexpr (!MASKED) {
           uint32_t y4[4] = {0u, 0u, 0u, 0u};
