@@ -438,7 +438,7 @@ def run_side_configs(args, world, rank, local) -> dict:
         "pairs_per_s": world * len(pairs) / (ms / 1e3), "kernels_per_batch": info["kernels"],
         "tensor_core_pairs": info["tensor_pairs"], "graph": True,
         "launches": [f"{g['pairs']} pairs row width {g['row_width']} tile {g['tile_rows']} rows "
-                     f"({g['tiles']} tiles)" for g in info["launches"]],
+                     f"sets of {g['set_size']} ({g['tiles']} tiles)" for g in info["launches"]],
         "plan_ms": plan_ms,
         "tuning": os.environ.get("IPB_AUTOTUNE", "groups (default)"),
         "roofline": {"bound": "tensor", "achieved": 2.0 * macs / (ms / 1e3) / 1e12,
@@ -725,6 +725,9 @@ def run_ours(args, world, rank, local):
     batch = device.Batch([(di, dt, m, dm) if masked else (di, dt, m) for m, masked in VARIANTS],
                          extremes=False)
     plan = device.BatchPlan(batch, tm.Precision.ExactFp64)
+    # the tuned launches: pairs on one image share a tile's A rows in sets
+    step_launches = [f"{g['pairs']} {'binary-mask' if g['masked'] else 'unmasked'} maps, tile {g['tile_rows']} "
+                     f"rows, sets of {g['set_size']} ({g['tiles']} tiles)" for g in plan.info()["launches"]]
 
     def step():
         plan.launch(stream)
@@ -842,6 +845,7 @@ def run_ours(args, world, rank, local):
         "config": bench_config(),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "step_launches": step_launches,
         "clocks": clk.summary(),
         "queries_per_s": world * len(VARIANTS) * args.steps / (ms / 1e3),
         "graph_ms_per_step": graph_ms / args.steps,

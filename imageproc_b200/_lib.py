@@ -119,6 +119,20 @@ def tensor_plan(w: int, h: int, masked: bool, batch: bool) -> dict | None:
     return {name: int(getattr(out, name)) for name, _ in TensorPlan._fields_}
 
 
+def tensor_set_plan(w: int, h: int, masked: bool, problems_per_set: int) -> dict | None:
+    """The tile plan of a batch group computing pairs on one image in sets of
+    `problems_per_set` (ipb_tensor_set_plan_for): host arithmetic. None when
+    no such plan fits."""
+    out = TensorPlan()
+    f = lib().ipb_tensor_set_plan_for
+    f.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_void_p]
+    st = f(w, h, int(bool(masked)), problems_per_set, C.byref(out))
+    if st == ERR_INVALID_ARGUMENT:
+        return None
+    check(st)
+    return {name: int(getattr(out, name)) for name, _ in TensorPlan._fields_}
+
+
 _lib = None
 
 u32 = C.c_uint32

@@ -101,13 +101,13 @@ struct TuneKey {
 struct GroupKey {
   uint32_t ks0;
   int masked;
-  uint32_t h8, wlog, mlog;
+  uint32_t h8, wlog, mlog, set;
   bool operator<(const GroupKey& o) const {
-    return std::tie(ks0, masked, h8, wlog, mlog) < std::tie(o.ks0, o.masked, o.h8, o.wlog, o.mlog);
+    return std::tie(ks0, masked, h8, wlog, mlog, set) < std::tie(o.ks0, o.masked, o.h8, o.wlog, o.mlog, o.set);
   }
 };
 struct GroupChoice {
-  uint32_t ks, nt;
+  uint32_t ks, nt, set;
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, bool> g_tune;
@@ -140,10 +140,12 @@ void tune_load_locked() {
       TuneKey k;
       int t;
       if (ls >> k.w >> k.h >> k.masked >> k.norm >> t) g_tune[k] = t != 0;
-    } else if (kind == "group") {
+    } else if (kind == "group2") {
       GroupKey k;
       GroupChoice c;
-      if (ls >> k.ks0 >> k.masked >> k.h8 >> k.wlog >> k.mlog >> c.ks >> c.nt) g_group_tune[k] = c;
+      if (ls >> k.ks0 >> k.masked >> k.h8 >> k.wlog >> k.mlog >> k.set >> c.ks >> c.nt >> c.set && c.set >= 1 &&
+          c.set <= kMaxSet)
+        g_group_tune[k] = c;
     }
   }
 }
@@ -158,11 +160,20 @@ void tune_store_locked() {
       out << "pair " << kv.first.w << ' ' << kv.first.h << ' ' << kv.first.masked << ' ' << kv.first.norm << ' '
           << (kv.second ? 1 : 0) << '\n';
     for (auto& kv : g_group_tune)
-      out << "group " << kv.first.ks0 << ' ' << kv.first.masked << ' ' << kv.first.h8 << ' ' << kv.first.wlog
-          << ' ' << kv.first.mlog << ' ' << kv.second.ks << ' ' << kv.second.nt << '\n';
+      out << "group2 " << kv.first.ks0 << ' ' << kv.first.masked << ' ' << kv.first.h8 << ' ' << kv.first.wlog
+          << ' ' << kv.first.mlog << ' ' << kv.first.set << ' ' << kv.second.ks << ' ' << kv.second.nt << ' '
+          << kv.second.set << '\n';
     if (!out) return;
   }
   std::rename(tmp.c_str(), f.c_str());  // whole files only, for processes sharing the file
+}
+
+// Largest set of pairs sharing an image that a launch computes together
+// (IPB_SET_MAX = 1..4; default 4; 1 computes every pair alone).
+uint32_t set_cap() {
+  const char* v = std::getenv("IPB_SET_MAX");
+  const int n = v ? std::atoi(v) : (int)kMaxSet;
+  return n < 1 ? 1u : (n > (int)kMaxSet ? kMaxSet : (uint32_t)n);
 }
 
 int autotune_mode() {  // 0: off, 1: groups, 2: groups and per-pair paths
@@ -246,10 +257,8 @@ ipb_status to_status(cudaError_t e, const char* what) {
 // caller re-arms the keys afterwards.
 template <class KeysOf>
 ipb_status tune_group(ipb_batch_plan* p, const std::vector<uint32_t>& mem, uint32_t ks0, bool masked, uint32_t hmax,
-                      KeysOf keys_of, GroupChoice& best) {
-  best = GroupChoice{ks0, 0};
-  uint32_t nts[2];
-  const uint32_t nnt = umma_tile_heights(masked, nts);
+                      uint32_t set, KeysOf keys_of, GroupChoice& best) {
+  best = GroupChoice{ks0, 0, 1};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   IPB_TRY(cudaEventCreate(&e0), "event");
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -258,16 +267,20 @@ ipb_status tune_group(ipb_batch_plan* p, const std::vector<uint32_t>& mem, uint3
   }
   float best_ms = 1e30f;
   cudaError_t err = cudaSuccess;
+  // sets of 1, 2 and the largest the pairs form; each with its tile heights
+  std::vector<uint32_t> sets{1u};
+  if (set >= 2) sets.push_back(2u);
+  if (set > 2) sets.push_back(set);
   for (uint32_t ks : {ks0, 2 * ks0}) {
+   for (uint32_t sz : sets) {
+    uint32_t nts[2];
+    const uint32_t nnt = umma_tile_heights(masked, sz, nts);
     for (uint32_t t = 0; t < nnt && err == cudaSuccess; ++t) {
       UmmaPlan pl;
-      if (!umma_plan_for(ks, masked, hmax, pl, nts[t])) continue;
+      if (!umma_plan_for(ks, masked, hmax, pl, nts[t], sz)) continue;
       std::vector<UmmaProblem> probs;
-      uint32_t tiles = 0;
-      for (uint32_t i : mem) {
-        probs.push_back(umma_problem(p->args[i], pl, tiles, keys_of(i)));
-        tiles += umma_problem_tiles(probs.back(), pl);
-      }
+      for (uint32_t i : mem) probs.push_back(umma_problem(p->args[i], pl, 0, keys_of(i)));
+      const uint32_t tiles = umma_make_sets(probs, pl);
       UmmaLaunch L{};
       UmmaProblem* d_probs = nullptr;
       if (probs.size() > kInlineProblems) {
@@ -297,9 +310,10 @@ ipb_status tune_group(ipb_batch_plan* p, const std::vector<uint32_t>& mem, uint3
       if (d_probs) cudaFree(d_probs);
       if (err == cudaSuccess && ms_best < best_ms) {
         best_ms = ms_best;
-        best = GroupChoice{ks, nts[t]};
+        best = GroupChoice{ks, nts[t], sz};
       }
     }
+   }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -494,15 +508,25 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
     if ((e = cudaMemset(p->d_sched, 0, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
   }
   auto keys_of = [&](uint32_t i) { return slot[i] >= 0 ? p->d_keys + 2 * slot[i] : nullptr; };
+  // the largest set the pairs `mem` form (pairs on one image with one
+  // template size), within the set cap
+  auto set_of = [&](const std::vector<uint32_t>& mem) {
+    std::vector<UmmaProblem> probs;
+    UmmaPlan any{};
+    for (uint32_t i : mem) probs.push_back(umma_problem(p->args[i], any, 0, nullptr));
+    return std::max(1u, std::min(umma_largest_set(probs), set_cap()));
+  };
   // each natural group's (row width, tile height): tuned, or the natural
   // width with the tallest tiles; groups that land on the same (width,
   // height, mask kind) share one launch
-  std::map<std::tuple<bool, uint32_t, uint32_t>, std::vector<uint32_t>> launches;
+  std::map<std::tuple<bool, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>> launches;
   for (auto& kv : by_key) {
     const std::vector<uint32_t>& mem = kv.second;
     const bool masked = p->args[mem.front()].mask != nullptr;
     const uint32_t ks0 = kv.first / 2;  // umma_group_key = row width * 2 + masked
-    GroupChoice c{ks0, 0};
+    const uint32_t set = set_of(mem);
+    // untuned: sets of up to four unmasked pairs, two binary-mask pairs
+    GroupChoice c{ks0, 0, masked ? std::min(set, 2u) : set};
     if (tune) {
       uint32_t hmax = 0, side = 0;
       double pos = 0;
@@ -512,7 +536,7 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
         side = std::max(side, std::max(a.W, a.H));
         pos += (double)(a.W - a.w + 1) * (a.H - a.h + 1);
       }
-      const GroupKey gk{ks0, masked ? 1 : 0, (hmax + 7) & ~7u, floor_log2(pos), floor_log2(side)};
+      const GroupKey gk{ks0, masked ? 1 : 0, (hmax + 7) & ~7u, floor_log2(pos), floor_log2(side), set};
       bool have = false;
       {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -524,14 +548,14 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
         }
       }
       if (!have) {
-        ipb_status st = tune_group(p, mem, ks0, masked, hmax, keys_of, c);
+        ipb_status st = tune_group(p, mem, ks0, masked, hmax, set, keys_of, c);
         if (st != IPB_OK) return fail(st);
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_group_tune[gk] = c;
         tune_store_locked();
       }
     }
-    auto& dst = launches[std::make_tuple(masked, c.ks, c.nt)];
+    auto& dst = launches[std::make_tuple(masked, c.ks, c.nt, c.set)];
     dst.insert(dst.end(), mem.begin(), mem.end());
   }
   for (auto& kv : launches) {
@@ -546,16 +570,14 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
       hmax = std::max(hmax, p->args[i].h);
       ks = std::max(ks, umma_row_width(p->args[i].w));
     }
-    // a cached choice that no longer fits falls back to the tallest tiles
-    if (!umma_plan_for(ks, masked, hmax, g.plan, nt) && !umma_plan_for(ks, masked, hmax, g.plan, 0))
+    // a cached choice that no longer fits falls back to the tallest tiles,
+    // then to problems alone
+    const uint32_t set = std::min(std::get<3>(kv.first), set_of(g.members));
+    if (!umma_plan_for(ks, masked, hmax, g.plan, nt, set) && !umma_plan_for(ks, masked, hmax, g.plan, 0, set) &&
+        !umma_plan_for(ks, masked, hmax, g.plan, 0, 1))
       return fail((ipb_status)report_error(IPB_ERR_CUDA, "no tensor-core plan"));
-    uint32_t tiles = 0;
-    for (uint32_t i : g.members) {
-      UmmaProblem q = umma_problem(p->args[i], g.plan, tiles, keys_of(i));
-      tiles += umma_problem_tiles(q, g.plan);
-      g.probs.push_back(q);
-    }
-    g.tiles = tiles;
+    for (uint32_t i : g.members) g.probs.push_back(umma_problem(p->args[i], g.plan, 0, keys_of(i)));
+    g.tiles = umma_make_sets(g.probs, g.plan);
     if (g.probs.size() > kInlineProblems) {
       if ((e = cudaMalloc(&g.d_probs, sizeof(UmmaProblem) * g.probs.size())) != cudaSuccess)
         return fail(to_status(e, "cudaMalloc"));
@@ -648,7 +670,8 @@ IPB_API ipb_status ipb_batch_plan_groups(const ipb_batch_plan* plan, uint32_t ma
   const uint32_t n = (uint32_t)plan->groups.size();
   for (uint32_t i = 0; i < n && i < max; ++i) {
     const ipb_batch_plan::Group& g = plan->groups[i];
-    out[i] = ipb_batch_group{g.plan.ks, g.plan.NT, g.plan.masked ? 1 : 0, (uint32_t)g.members.size(), g.tiles};
+    out[i] = ipb_batch_group{g.plan.ks, g.plan.NT, g.plan.masked ? 1 : 0, (uint32_t)g.members.size(), g.tiles,
+                             g.plan.set_max};
   }
   if (count) *count = n;
   return IPB_OK;

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <mutex>
 #include <cuda_runtime.h>
 
@@ -197,9 +198,17 @@ struct UmmaProblem {
   uint32_t Wo, Ho, tiles_x, tile_begin;  // tile_begin: first global tile of the problem
   uint32_t kmma, zrows, rows_max, load_mode;
   int method, precision;
+  // Problems on one image with one template size may form a set that the
+  // kernel computes tile by tile together, sharing the staged image rows and
+  // the A operand built from them (each member keeps its own template side,
+  // accumulators, MMAs and epilogue). On a set's first problem: the number of
+  // members (1 for a problem alone); 0 on the others, which follow it in the
+  // problem list and carry its tile_begin. Tiles are counted per set.
+  uint32_t set_n;
 };
 
 constexpr uint32_t kInlineProblems = 8;  // problems passed in the kernel parameters
+constexpr uint32_t kMaxSet = 4;          // problems per set
 
 struct UmmaLaunch {
   UmmaProblem inl[kInlineProblems];
@@ -207,6 +216,7 @@ struct UmmaLaunch {
   uint32_t nprobs, tiles;
   uint32_t NT, rps, imgp, plane_bytes, nbuf;
   uint32_t z_off, img_off, rs_off;
+  uint32_t set_max;  // largest set: accumulators and template buffers reserved per member
   unsigned int* err;
   unsigned int tag;
   // budget of the pipeline's bounded waits, per tile (pipeline_wait_ns())
@@ -224,6 +234,7 @@ struct UmmaPlan {
   uint32_t ks;
   bool masked;
   uint32_t NT, rps, imgp, plane_bytes, nbuf, z_off, img_off, rs_off, smem;
+  uint32_t set_max;  // problems per set the plan holds (1..kMaxSet)
 };
 
 uint32_t umma_group_key(const MatchArgs& a);  // natural row width * 2 + masked
@@ -232,11 +243,20 @@ uint32_t umma_row_width(uint32_t w);
 // Sets every tensor-core kernel's shared-memory limit (outside stream capture).
 cudaError_t umma_prepare_kernels();
 // Plan of a batch group (launches of many tiles): row width ks (8..64, a
-// power of two; 32 at most with a mask) and the tile height nt, or the
-// tallest tiles that fit when nt is 0. False when no plan fits.
-bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt = 0);
-// The tile heights a batch group can use, tallest first; returns the count.
-uint32_t umma_tile_heights(bool masked, uint32_t out[2]);
+// power of two; 32 at most with a mask), sets of up to `set` problems
+// (1..kMaxSet) and the tile height nt, or the tallest tiles that fit when nt
+// is 0. False when no plan fits.
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt = 0, uint32_t set = 1);
+// The tile heights a batch group with sets of up to `set` problems can use,
+// tallest first; returns the count.
+uint32_t umma_tile_heights(bool masked, uint32_t set, uint32_t out[2]);
+// Problems of a launch that share an image and a template size (and the mask
+// kind): the size of the largest such class, at most kMaxSet.
+uint32_t umma_largest_set(const std::vector<UmmaProblem>& probs);
+// Reorders a launch's problems so that each class of the above follows
+// itself, cuts the classes into sets of at most pl.set_max problems and
+// numbers the sets' tiles from 0; returns the launch's tile count.
+uint32_t umma_make_sets(std::vector<UmmaProblem>& probs, const UmmaPlan& pl);
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
                          unsigned long long* ext_keys);
 uint32_t umma_problem_tiles(const UmmaProblem& q, const UmmaPlan& pl);

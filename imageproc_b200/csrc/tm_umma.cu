@@ -55,6 +55,10 @@
 // Every wait is bounded (2 s); a wait that runs out records the launch's tag
 // in the error word and the CTA leaves its loop, drains its MMAs and frees its
 // tensor memory.
+#include <algorithm>
+#include <tuple>
+#include <vector>
+
 #include "tm_common.cuh"
 #include "tm_internal.h"
 #include "tm_sm100.cuh"
@@ -88,12 +92,28 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, uint32_
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// problem index of a global tile, advancing monotonically from `pi`
+// first problem of the set that owns a global tile, advancing monotonically
+// from the set starting at `pi`
 __device__ __forceinline__ uint32_t find_problem(const UmmaLaunch& L, const UmmaProblem* P, uint32_t pi,
                                                  uint32_t tile) {
-  while (pi + 1 < L.nprobs && tile >= P[pi + 1].tile_begin) ++pi;
-  return pi;
+  for (;;) {
+    const uint32_t nx = pi + max(P[pi].set_n, 1u);
+    if (nx >= L.nprobs || tile < P[nx].tile_begin) return pi;
+    pi = nx;
+  }
 }
+
+// Template side cached in shared memory per set member slot: the Z buffers
+// and TSS stay valid while the slot's template, mask and shape are unchanged
+// (consecutive tiles of one set; sets that repeat a template).
+struct ZKey {
+  const uint8_t* tpl;
+  const uint8_t* mask;
+  uint32_t w, h, kmma, pad;
+};
+// shared-memory header below the band table: barriers and flags (0..255),
+// TSS partial sums per member and warp, TSS per member, the members' keys
+static_assert(256 + kMaxSet * kWarps * 8 + 64 + kMaxSet * sizeof(ZKey) <= kBandTable, "kernel header");
 
 // Stage image rows [y0, y0 + nrows) x columns [x0, x0 + imgp) of plane 0 for
 // the problem's local tile, zero past the right edge. Asynchronous unless the
@@ -335,7 +355,54 @@ __device__ __forceinline__ void umma_epilogue_dispatch(const UmmaEpi& e, int met
   }
 }
 
-template <int KS, bool MASKED>
+// The MMAs of one pipeline stage, issued by the elected lane: for each of
+// the stage's cnt image rows (reading four band entries {n0, idesc, first Z
+// row} ahead of their MMAs; the reads run at most three entries past the
+// tile's last row, still inside shared memory since the Z buffers follow the
+// table, and are unused), each of the set's NS members multiplies the row's
+// A (tensor memory) by its own template side (Z, shared memory) into its own
+// accumulators over the row's band of output rows.
+struct StageIssue {
+  const uint4* band;
+  uint32_t r0, cnt, a_stage, a_row_cols, dlo, dhi, zslot16, zoff1, kstride, ksteps, tmem, acc_cols, NT, ymask;
+};
+
+template <int NS, int KS, bool MASKED>
+__device__ __forceinline__ void issue_stage(const StageIssue& si) {
+  constexpr int NCORR = MASKED ? 3 : 1;  // correlations, one per plane
+  for (uint32_t i0 = 0; i0 < si.cnt; i0 += 4) {
+    uint4 bd[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bd[j] = si.band[si.r0 + i0 + j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (i0 + j < si.cnt) {
+        const uint32_t n0 = bd[j].x, idesc = bd[j].y;
+        const uint32_t zrow = si.dlo + bd[j].z;
+        const uint32_t a = si.a_stage + (i0 + j) * si.a_row_cols;
+#pragma unroll
+        for (int p = 0; p < NS; ++p) {
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c) {
+            if (c > 0 && !((si.ymask >> p) & 1u)) break;  // masked CrossCorrelation: X alone
+            const uint32_t zo = zrow + p * si.zslot16 + c * si.zoff1;
+            const uint32_t acc = p * si.acc_cols + (c == 0 ? 0u : si.NT);  // X, or Y for both parts of I^2
+#pragma unroll
+            for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
+              if (kk < si.ksteps)
+                mma_i8_ts(si.tmem + acc + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                          ((uint64_t)si.dhi << 32) | (zo + kk * si.kstride), idesc, 1u);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// SETS: launches whose plan holds sets of two or more problems; the instance
+// for problems alone compiles the member loops away.
+template <int KS, bool MASKED, bool SETS>
 __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_constant__ UmmaLaunch L) {
   constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, I^2 mod 255, floor(I^2 / 255))
   constexpr int NCORR = MASKED ? 3 : 1;  // correlations, one per plane
@@ -349,7 +416,10 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + 128);
   volatile int* s_err = reinterpret_cast<volatile int*>(smem + 132);
   volatile uint32_t* s_next = reinterpret_cast<volatile uint32_t*>(smem + 136);  // tile after the current one
-  unsigned long long* s_part = reinterpret_cast<unsigned long long*>(smem + 256);  // kWarps partial sums
+  // [kMaxSet][kWarps] partial sums of TSS, per member slot: TSS, Z keys
+  unsigned long long* s_part = reinterpret_cast<unsigned long long*>(smem + 256);
+  uint32_t* s_tss = reinterpret_cast<uint32_t*>(smem + 256 + kMaxSet * kWarps * 8);
+  ZKey* s_zkey = reinterpret_cast<ZKey*>(smem + 256 + kMaxSet * kWarps * 8 + 64);
   uint8_t* zbuf = smem + L.z_off;
   uint8_t* s_img = smem + L.img_off;
   uint32_t* s_rs = reinterpret_cast<uint32_t*>(smem + L.rs_off);
@@ -366,6 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     mbar_init(dfull, 1);
     mbar_init(drain, 1);
     *s_err = 0;
+    for (uint32_t p = 0; p < kMaxSet; ++p) s_zkey[p] = ZKey{nullptr, nullptr, 0u, 0u, 0u, 0u};
     mbar_init_fence();
   }
   if (mma_warp) {
@@ -382,18 +453,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  const uint32_t a_col0 = NACC * L.NT;
+  const uint32_t acc_cols = NACC * L.NT;  // accumulator columns per set member
+  const uint32_t a_col0 = (SETS ? L.set_max : 1u) * acc_cols;
   const uint32_t a_row_cols = NPL * KS;
 
   uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
   uint32_t tcount = 0;       // tiles finished by this CTA
-  // template side whose Z buffers and TSS are in shared memory (consecutive
-  // problems of a batch often share it: several methods of one pair, one
-  // template over several images)
-  const uint8_t* z_tpl = nullptr;
-  const uint8_t* z_mask = nullptr;
-  uint32_t z_w = 0, z_h = 0, z_kmma = 0;
-  uint32_t tss = 0;
   bool ok = true;
 
   for (uint32_t tile = blockIdx.x, next = 0; tile < L.tiles; tile = next, ++tcount) {
@@ -415,14 +480,29 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
     const uint32_t y0 = (lt / q.tiles_x) * L.NT;
     const uint32_t nrows = min(q.rows_max, q.H - y0);
     const uint32_t zplane = (q.kmma / 16) * q.zrows * 16;
-    const bool new_z = q.tpl != z_tpl || q.mask != z_mask || q.w != z_w || q.h != z_h || q.kmma != z_kmma;
-    if (new_z) {
-      // Z buffers, K-chunk-major: chunk c holds rows j = 0..zrows-1 of 16 bytes,
-      // row j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
+    const uint32_t zslot = NZ * zplane;  // template-side bytes per set member
+    const uint32_t nset = SETS ? max(q.set_n, 1u) : 1u;
+    // members whose template side is not cached in their slot; the members
+    // share the image, the template size and therefore the band table
+    uint32_t zbits = 0;
+    for (uint32_t p = 0; p < nset; ++p) {
+      const UmmaProblem& mp = P[pi + p];
+      const ZKey k = s_zkey[p];
+      if (mp.tpl != k.tpl || mp.mask != k.mask || mp.w != k.w || mp.h != k.h || mp.kmma != k.kmma)
+        zbits |= 1u << p;
+    }
+    if (zbits) {
+      // Z buffers of every member to rebuild, in one pass over all of them:
+      // K-chunk-major, chunk c holds rows j = 0..zrows-1 of 16 bytes, row
+      // j = template row h-1-(j-16) for 16 <= j < h+16, else zero.
       //   unmasked: Z_0 from T;  binary mask: Z_0 from T*m, Z_1 from m, Z_2 from 255*m
-      const uint32_t nchunks = q.kmma / 16;
-      for (uint32_t idx = threadIdx.x; idx < NZ * nchunks * q.zrows; idx += kThreads) {
-        const uint32_t zp = idx / (nchunks * q.zrows);
+      const uint32_t nchunks = q.kmma / 16, per = NZ * nchunks * q.zrows;
+      for (uint32_t idx = threadIdx.x; idx < nset * per; idx += kThreads) {
+        const uint32_t p = idx / per;
+        if (!((zbits >> p) & 1u)) continue;
+        const uint8_t* tp = P[pi + p].tpl;
+        const uint8_t* mk = P[pi + p].mask;
+        const uint32_t zp = (idx % per) / (nchunks * q.zrows);
         const uint32_t rem = idx % (nchunks * q.zrows);
         const uint32_t c = rem / q.zrows, j = rem % q.zrows;
         uint32_t wd[4] = {0u, 0u, 0u, 0u};
@@ -434,18 +514,35 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
             if (dx < q.w) {
               uint32_t v;
               if constexpr (MASKED) {
-                const uint32_t mv = __ldg(q.mask + row + dx);
-                v = zp == 0 ? (uint32_t)__ldg(q.tpl + row + dx) * mv : (zp == 1 ? mv : 255u * mv);
+                const uint32_t mv = __ldg(mk + row + dx);
+                v = zp == 0 ? (uint32_t)__ldg(tp + row + dx) * mv : (zp == 1 ? mv : 255u * mv);
               } else {
-                v = __ldg(q.tpl + row + dx);
+                v = __ldg(tp + row + dx);
               }
               wd[k >> 2] |= (v & 0xFFu) << (8 * (k & 3));
             }
           }
         }
-        *reinterpret_cast<uint4*>(zbuf + zp * zplane + (size_t)(c * q.zrows + j) * 16) =
+        *reinterpret_cast<uint4*>(zbuf + p * zslot + zp * zplane + (size_t)(c * q.zrows + j) * 16) =
             make_uint4(wd[0], wd[1], wd[2], wd[3]);
       }
+      // TSS = sum (T*m)^2 (m = 1 unmasked) of each rebuilt member, exact;
+      // per-warp partials in shared memory
+      for (uint32_t p = 0; p < nset; ++p) {
+        if (!((zbits >> p) & 1u)) continue;
+        const uint8_t* tp = P[pi + p].tpl;
+        const uint8_t* mk = P[pi + p].mask;
+        unsigned long long t2 = 0;
+        for (uint32_t k = threadIdx.x; k < q.w * q.h; k += kThreads) {
+          uint32_t t = __ldg(tp + k);
+          if constexpr (MASKED) t *= __ldg(mk + k);
+          t2 += (unsigned long long)t * t;
+        }
+        for (int o = 16; o > 0; o >>= 1) t2 += __shfl_down_sync(0xffffffffu, t2, o);
+        if (lane == 0) s_part[p * kWarps + warp] = t2;
+      }
+    }
+    if (zbits) {
       // the MMA band of every image row r of a tile: image row r feeds output
       // rows n in [r-h+1, r], rounded out to 16 (rows past the map are computed,
       // not stored): {first accumulator column n0, instruction descriptor with
@@ -456,33 +553,29 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         const uint32_t idesc = (idesc_u8u8_s32(kM, 16) & ~(0x3Fu << 17)) | (((n1 - n0) >> 3) << 17);
         reinterpret_cast<uint4*>(smem + kBandTable)[r] = make_uint4(n0, idesc, n0 + q.h + 15u - r, 0u);
       }
-      // TSS = sum (T*m)^2 (m = 1 unmasked), exact; per-warp partials in shared memory
-      unsigned long long t2 = 0;
-      for (uint32_t k = threadIdx.x; k < q.w * q.h; k += kThreads) {
-        uint32_t t = __ldg(q.tpl + k);
-        if constexpr (MASKED) t *= __ldg(q.mask + k);
-        t2 += (unsigned long long)t * t;
-      }
-      for (int o = 16; o > 0; o >>= 1) t2 += __shfl_down_sync(0xffffffffu, t2, o);
-      if (lane == 0) s_part[warp] = t2;
       fence_proxy_async_smem();
     }
     cp_async_wait_all();
     __syncthreads();
     if (*s_err) break;
     next = *s_next;
-    if (new_z) {
-      unsigned long long t = 0;
-      for (int k = 0; k < kWarps; ++k) t += s_part[k];
-      tss = (uint32_t)t;  // < 2^31: at most 33025 template pixels
-      z_tpl = q.tpl;
-      z_mask = q.mask;
-      z_w = q.w;
-      z_h = q.h;
-      z_kmma = q.kmma;
+    if (zbits && threadIdx.x == 0) {
+      // every thread has read the slots' keys above, before the barrier
+      for (uint32_t p = 0; p < nset; ++p) {
+        if (!((zbits >> p) & 1u)) continue;
+        unsigned long long t = 0;
+        for (int k = 0; k < kWarps; ++k) t += s_part[p * kWarps + k];
+        s_tss[p] = (uint32_t)t;  // < 2^31: at most 33025 template pixels
+        const UmmaProblem& mp = P[pi + p];
+        s_zkey[p] = ZKey{mp.tpl, mp.mask, mp.w, mp.h, mp.kmma, 0u};
+      }
     }
-    // masked CrossCorrelation scores X alone: no Y correlations, no I^2 planes
-    const bool need_y = !MASKED || q.method != kCcorr;
+    // masked CrossCorrelation scores X alone: its members skip the Y
+    // correlations, and a set of such members skips the I^2 planes
+    uint32_t ymask = 0;  // members that need Y
+    for (uint32_t p = 0; p < nset; ++p)
+      if (!MASKED || P[pi + p].method != kCcorr) ymask |= 1u << p;
+    const bool need_y = ymask != 0;
     if (MASKED && need_y) {
       // the two u8 parts of I^2 (I^2 mod 255, floor(I^2 / 255)) next to the
       // staged image
@@ -527,10 +620,11 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t ncols = 16 * ((sub + 1) * chunks / kSubs) - c_begin;
       {
         const uint32_t zero16[16] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        for (uint32_t p = 0; p < nset; ++p)
 #pragma unroll
-        for (int c = 0; c < NACC; ++c)
-          for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
-            tmem_st16(tmem_addr(tmem, lane_base, c * L.NT + col), zero16);
+          for (int c = 0; c < NACC; ++c)
+            for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
+              tmem_st16(tmem_addr(tmem, lane_base, p * acc_cols + c * L.NT + col), zero16);
       }
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
@@ -575,8 +669,14 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
           for (; r < c_begin + q.h; ++r) y4[0] += r < nrows ? s_rs[r * kM + m] : 0u;
           Y = y4[0] + y4[1] + y4[2] + y4[3];
         }
-        const UmmaEpi e{&q, tmem, lane_base, c_begin, ncols, L.NT, nrows, m, x, y0, tss, (uint32_t)lane, s_rs, Y};
-        umma_epilogue_dispatch<MASKED>(e, q.method, q.precision == IPB_PRECISION_EXACT_FP64, q.ext != nullptr);
+        // each member's scores from its own accumulators (Y is the members'
+        // common window sum of I^2, unmasked)
+        for (uint32_t p = 0; p < nset; ++p) {
+          const UmmaProblem qp = P[pi + p];
+          const UmmaEpi e{&qp, tmem + p * acc_cols, lane_base, c_begin, ncols, L.NT, nrows, m, x, y0, s_tss[p],
+                          (uint32_t)lane, s_rs, Y};
+          umma_epilogue_dispatch<MASKED>(e, qp.method, qp.precision == IPB_PRECISION_EXACT_FP64, qp.ext != nullptr);
+        }
       }
       if (!ok) {
         *s_err = 1;
@@ -588,6 +688,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint64_t desc0 = smem_desc_noswizzle(smem_u32(zbuf), q.zrows * 16, 128);
       const uint32_t dlo = (uint32_t)desc0, dhi = (uint32_t)(desc0 >> 32);
       const uint32_t zoff1 = zplane >> 4;
+      const uint32_t zslot16 = zslot >> 4;   // one member's template side, in 16-byte units
       const uint32_t kstride = 2u * q.zrows;  // one 32-byte K step of Z, in 16-byte units
       const uint32_t ksteps = q.kmma / 32;
       const uint4* band = reinterpret_cast<const uint4*>(smem + kBandTable);
@@ -605,34 +706,17 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         const uint32_t r0 = st * L.rps, cnt = min(nrows, r0 + L.rps) - r0;
         const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
         if (leader) {
-          // the elected lane alone walks the stage's rows, reading four band
-          // entries {n0, idesc, first Z row} ahead of their MMAs. The reads
-          // run at most three entries past the tile's last row: still inside
-          // shared memory (the Z buffers follow the table), and unused.
-          for (uint32_t i0 = 0; i0 < cnt; i0 += 4) {
-            uint4 bd[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) bd[j] = band[r0 + i0 + j];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              if (i0 + j < cnt) {
-                const uint32_t n0 = bd[j].x, idesc = bd[j].y;
-                const uint32_t zrow = dlo + bd[j].z;
-                const uint32_t a = a_stage + (i0 + j) * a_row_cols;
-#pragma unroll
-                for (int c = 0; c < NCORR; ++c) {
-                  if (c > 0 && !need_y) break;
-                  const uint32_t zo = zrow + c * zoff1;
-                  const uint32_t acc = c == 0 ? 0u : 1u;  // X, or Y for both parts of I^2
-#pragma unroll
-                  for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
-                    if (kk < ksteps)
-                      mma_i8_ts(tmem + acc * L.NT + n0, a + (MASKED ? c * KS : 0) + kk * 8,
-                                ((uint64_t)dhi << 32) | (zo + kk * kstride), idesc, 1u);
-                  }
-                }
-              }
+          const StageIssue si{band, r0, cnt, a_stage, a_row_cols, dlo, dhi, zslot16, zoff1, kstride, ksteps,
+                              tmem, acc_cols, L.NT, ymask};
+          if constexpr (SETS) {
+            switch (nset) {
+              case 1: issue_stage<1, KS, MASKED>(si); break;
+              case 2: issue_stage<2, KS, MASKED>(si); break;
+              case 3: issue_stage<3, KS, MASKED>(si); break;
+              default: issue_stage<4, KS, MASKED>(si); break;
             }
+          } else {
+            issue_stage<1, KS, MASKED>(si);
           }
           mma_commit(&empty[s]);
         }
@@ -668,21 +752,29 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   }
 }
 
-template <int KS, bool MASKED>
+template <int KS, bool MASKED, bool SETS>
 cudaError_t launch_ks(const UmmaLaunch& L, uint32_t smem, uint32_t grid, cudaStream_t s) {
   static PerDeviceOnce attr;  // per instantiation and device
   cudaError_t e = attr.run([] {
-    return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED, SETS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 227 * 1024);
   });
   if (e != cudaSuccess) return e;
-  umma_match_kernel<KS, MASKED><<<grid, kThreads, smem, s>>>(L);
+  umma_match_kernel<KS, MASKED, SETS><<<grid, kThreads, smem, s>>>(L);
   return cudaGetLastError();
 }
 
 template <int KS, bool MASKED>
+cudaError_t launch_ks2(const UmmaLaunch& L, uint32_t smem, uint32_t grid, cudaStream_t s) {
+  return L.set_max > 1 ? launch_ks<KS, MASKED, true>(L, smem, grid, s) : launch_ks<KS, MASKED, false>(L, smem, grid, s);
+}
+
+template <int KS, bool MASKED>
 cudaError_t set_smem_attr() {
-  return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(umma_match_kernel<KS, MASKED, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(umma_match_kernel<KS, MASKED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               227 * 1024);
 }
 
@@ -698,23 +790,44 @@ uint32_t ks_of(uint32_t w) {
 // Kernel-wide tile and shared-memory plan for a group sharing (ks, masked):
 // sized for the group's tallest template.
 // nt_only: a tile height the plan must use (0: the tallest that fits).
-bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl, uint32_t nt_only = 0) {
+// Tile heights, tallest first, for sets of up to `set` problems: a tile of
+// NT output rows reads NT + h - 1 image rows, so taller tiles repeat fewer
+// rows, while each member's accumulators (NT columns, two with a mask) leave
+// less tensor memory for the A stages. Binary-mask tiles of 96 rows (`tall`:
+// launches of many tiles, where throughput counts) only where a stage still
+// holds 3 image rows; a launch of one map or one row band ends after about
+// one tile's time, which the 64-row tile keeps shorter. Sets trade tile
+// height for members: the A rows of a tile serve every member.
+uint32_t tile_heights(bool masked, bool tall, uint32_t set, uint32_t out[2]) {
+  if (set <= 1) {
+    out[0] = masked ? (tall ? 96u : 64u) : 128u;
+    out[1] = 64u;
+  } else if (set == 2) {
+    out[0] = masked ? 64u : 128u;
+    out[1] = masked ? 32u : 64u;
+  } else {
+    out[0] = masked ? 32u : 64u;
+    out[1] = masked ? 16u : 32u;
+  }
+  return 2;
+}
+
+bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl, uint32_t nt_only = 0,
+               uint32_t set = 1) {
+  if (set < 1 || set > kMaxSet) return false;
   const uint32_t npl = masked ? 3 : 1, nacc = masked ? 2 : 1, nz = masked ? 3 : 1;
   pl.ks = ks;
   pl.masked = masked;
+  pl.set_max = set;
   pl.imgp = kM + 4 * ks + 16;
   const uint32_t kmma = 4 * ks;  // largest K of the group
   const uint32_t zplane = (kmma / 16) * (hmax + 32) * 16;
-  // tile heights, tallest first: a tile of NT output rows reads NT + h - 1
-  // image rows, so taller tiles repeat fewer rows, while the accumulators
-  // leave less tensor memory for the A stages. Binary-mask tiles of 96 rows
-  // (`tall`: launches of many tiles, where throughput counts) only where a
-  // stage still holds 3 image rows; a launch of one map or one row band ends
-  // after about one tile's time, which the 64-row tile keeps shorter.
-  const uint32_t nts[2] = {masked ? (tall ? 96u : 64u) : 128u, 64u};
+  uint32_t nts[2];
+  tile_heights(masked, tall, set, nts);
   for (uint32_t nt : nts) {
     if (nt_only && nt != nt_only) continue;
-    const uint32_t tm_left = kTmemCols - nacc * nt;
+    if (set * nacc * nt >= kTmemCols) continue;
+    const uint32_t tm_left = kTmemCols - set * nacc * nt;
     const uint32_t rps = tm_left / (kStages * npl * ks);
     if (rps < 1) continue;
     if (masked && nt > 64 && rps < 3) continue;
@@ -722,7 +835,7 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl,
     const uint32_t plane = (uint32_t)align_up((size_t)rows * pl.imgp, 128);
     for (uint32_t nbuf : {2u, 1u}) {
       const uint32_t z_off = kSmemHeader;
-      const uint32_t img_off = z_off + (uint32_t)align_up((size_t)nz * zplane, 128);
+      const uint32_t img_off = z_off + (uint32_t)align_up((size_t)set * nz * zplane, 128);
       const uint32_t rs_off = img_off + nbuf * npl * plane;
       const uint32_t end = rs_off + (masked ? 0u : rows * kM * 4);
       if (end <= 227u * 1024u) {
@@ -771,15 +884,59 @@ cudaError_t umma_prepare_kernels() {
   return cudaSuccess;
 }
 
-bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt) {
+bool umma_plan_for(uint32_t ks, bool masked, uint32_t hmax, UmmaPlan& pl, uint32_t nt, uint32_t set) {
   if (ks < 8 || ks > (masked ? 32u : 64u) || (ks & (ks - 1))) return false;
-  return make_plan(ks, masked, hmax, /*tall=*/true, pl, nt);
+  return make_plan(ks, masked, hmax, /*tall=*/true, pl, nt, set);
 }
 
-uint32_t umma_tile_heights(bool masked, uint32_t out[2]) {
-  out[0] = masked ? 96u : 128u;
-  out[1] = 64u;
-  return 2;
+uint32_t umma_tile_heights(bool masked, uint32_t set, uint32_t out[2]) {
+  return tile_heights(masked, /*tall=*/true, set, out);
+}
+
+namespace {
+// the class a problem's set is drawn from: one image, one template size, one mask kind
+bool same_class(const UmmaProblem& a, const UmmaProblem& b) {
+  return a.img == b.img && a.W == b.W && a.H == b.H && a.w == b.w && a.h == b.h &&
+         (a.mask != nullptr) == (b.mask != nullptr);
+}
+bool class_less(const UmmaProblem& a, const UmmaProblem& b) {
+  return std::tie(a.img, a.W, a.H, a.w, a.h) < std::tie(b.img, b.W, b.H, b.w, b.h);
+}
+}  // namespace
+
+uint32_t umma_largest_set(const std::vector<UmmaProblem>& probs) {
+  std::vector<UmmaProblem> v(probs);
+  std::stable_sort(v.begin(), v.end(), class_less);
+  uint32_t best = v.empty() ? 0u : 1u;
+  for (size_t i = 0, j; i < v.size(); i = j) {
+    for (j = i + 1; j < v.size() && same_class(v[i], v[j]); ++j) {
+    }
+    best = std::max(best, (uint32_t)(j - i));
+  }
+  return std::min(best, kMaxSet);
+}
+
+uint32_t umma_make_sets(std::vector<UmmaProblem>& probs, const UmmaPlan& pl) {
+  std::stable_sort(probs.begin(), probs.end(), class_less);
+  uint32_t tiles = 0;
+  for (size_t i = 0, j; i < probs.size(); i = j) {
+    for (j = i + 1; j < probs.size() && same_class(probs[i], probs[j]); ++j) {
+    }
+    // a class of cnt problems in nsets sets whose sizes differ by at most one
+    const uint32_t cnt = (uint32_t)(j - i), cap = std::max(pl.set_max, 1u);
+    const uint32_t nsets = (cnt + cap - 1) / cap;
+    size_t k = i;
+    for (uint32_t t = 0; t < nsets; ++t) {
+      const uint32_t sz = cnt / nsets + (t < cnt % nsets ? 1u : 0u);
+      for (uint32_t u = 0; u < sz; ++u) {
+        probs[k + u].set_n = u == 0 ? sz : 0u;
+        probs[k + u].tile_begin = tiles;
+      }
+      tiles += umma_problem_tiles(probs[k], pl);
+      k += sz;
+    }
+  }
+  return tiles;
 }
 
 UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_begin,
@@ -805,6 +962,7 @@ UmmaProblem umma_problem(const MatchArgs& a, const UmmaPlan& pl, uint32_t tile_b
   q.load_mode = ((ia & 15u) == 0 && (a.W & 15u) == 0) ? 2 : (((ia & 3u) == 0 && (a.W & 3u) == 0) ? 1 : 0);
   q.method = a.method;
   q.precision = a.precision;
+  q.set_n = 1;
   return q;
 }
 
@@ -821,22 +979,23 @@ cudaError_t launch_umma_batch(const UmmaPlan& pl, UmmaLaunch& L, cudaStream_t st
   L.z_off = pl.z_off;
   L.img_off = pl.img_off;
   L.rs_off = pl.rs_off;
+  L.set_max = pl.set_max;
   if (L.tiles == 0) return cudaSuccess;
   const uint32_t grid = L.tiles < (uint32_t)sm_count() ? L.tiles : (uint32_t)sm_count();
   cudaError_t e;
   timer_begin(timer, kKernelUmma, stream);
   if (pl.masked) {
     switch (pl.ks) {
-      case 8: e = launch_ks<8, true>(L, pl.smem, grid, stream); break;
-      case 16: e = launch_ks<16, true>(L, pl.smem, grid, stream); break;
-      default: e = launch_ks<32, true>(L, pl.smem, grid, stream); break;
+      case 8: e = launch_ks2<8, true>(L, pl.smem, grid, stream); break;
+      case 16: e = launch_ks2<16, true>(L, pl.smem, grid, stream); break;
+      default: e = launch_ks2<32, true>(L, pl.smem, grid, stream); break;
     }
   } else {
     switch (pl.ks) {
-      case 8: e = launch_ks<8, false>(L, pl.smem, grid, stream); break;
-      case 16: e = launch_ks<16, false>(L, pl.smem, grid, stream); break;
-      case 32: e = launch_ks<32, false>(L, pl.smem, grid, stream); break;
-      default: e = launch_ks<64, false>(L, pl.smem, grid, stream); break;
+      case 8: e = launch_ks2<8, false>(L, pl.smem, grid, stream); break;
+      case 16: e = launch_ks2<16, false>(L, pl.smem, grid, stream); break;
+      case 32: e = launch_ks2<32, false>(L, pl.smem, grid, stream); break;
+      default: e = launch_ks2<64, false>(L, pl.smem, grid, stream); break;
     }
   }
   count_launch(kKernelUmma);
@@ -850,17 +1009,21 @@ cudaError_t launch_umma_extremes(const uint8_t* img, uint32_t W, uint32_t H, con
                                  cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   if (n > kInlineProblems || !umma_shape_ok(w, h, false)) return cudaErrorNotSupported;
+  // the templates share the image: sets of up to kMaxSet share its A rows
+  const uint32_t nsets = (n + kMaxSet - 1) / kMaxSet, set = (n + nsets - 1) / nsets;
   UmmaPlan pl;
-  if (!make_plan(ks_of(w), false, h, /*tall=*/true, pl)) return cudaErrorNotSupported;
+  if (!make_plan(ks_of(w), false, h, /*tall=*/true, pl, 0, set) && !make_plan(ks_of(w), false, h, true, pl, 0, 1))
+    return cudaErrorNotSupported;
   cudaError_t e = umma_prepare_kernels();
   if (e != cudaSuccess) return e;
-  UmmaLaunch L{};
-  uint32_t tiles = 0;
+  std::vector<UmmaProblem> probs;
   for (uint32_t i = 0; i < n; ++i) {
     const MatchArgs a{img, W, H, tpls[i], w, h, nullptr, false, method, precision, nullptr, stream};
-    L.inl[i] = umma_problem(a, pl, tiles, keys + 2 * i);
-    tiles += umma_problem_tiles(L.inl[i], pl);
+    probs.push_back(umma_problem(a, pl, 0, keys + 2 * i));
   }
+  const uint32_t tiles = umma_make_sets(probs, pl);
+  UmmaLaunch L{};
+  for (uint32_t i = 0; i < n; ++i) L.inl[i] = probs[i];
   L.nprobs = n;
   L.tiles = tiles;
   L.err = err_word;
@@ -937,6 +1100,28 @@ cudaError_t launch_extremes_keys_finish(unsigned long long* keys, const uint32_t
 }  // namespace ipb
 
 #define IPB_API extern "C" __attribute__((visibility("default")))
+
+IPB_API ipb_status ipb_tensor_set_plan_for(uint32_t w, uint32_t h, int masked, uint32_t problems_per_set,
+                                           ipb_tensor_plan* out) {
+  using namespace ipb;
+  if (!out) return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!umma_shape_ok(w, h, masked != 0))
+    return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "template shape not taken by the tensor path");
+  if (problems_per_set < 1 || problems_per_set > kMaxSet)
+    return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "problems per set outside 1..4");
+  UmmaPlan pl;
+  if (!make_plan(ks_of(w), masked != 0, h, /*tall=*/true, pl, 0, problems_per_set))
+    return (ipb_status)report_error(IPB_ERR_INVALID_ARGUMENT, "no tensor-core plan fits this template");
+  const uint32_t planes = masked ? 3u : 1u, accumulators = masked ? 2u : 1u;
+  out->tile_rows = pl.NT;
+  out->image_rows = pl.NT + h - 1;
+  out->rows_per_stage = pl.rps;
+  out->stages = kStages;
+  out->image_buffers = pl.nbuf;
+  out->tmem_columns = problems_per_set * accumulators * pl.NT + kStages * planes * pl.ks * pl.rps;
+  out->smem_bytes = pl.smem;
+  return IPB_OK;
+}
 
 IPB_API ipb_status ipb_tensor_plan_for(uint32_t w, uint32_t h, int masked, int batch, ipb_tensor_plan* out) {
   using namespace ipb;

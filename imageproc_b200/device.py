@@ -91,7 +91,7 @@ EXTREMES_DTYPE = [("max_value", "<f4"), ("min_value", "<f4"), ("max_x", "<u4"), 
 
 class _BatchGroup(C.Structure):
     _fields_ = [("row_width", C.c_uint32), ("tile_rows", C.c_uint32), ("masked", C.c_int),
-                ("pairs", C.c_uint32), ("tiles", C.c_uint32)]
+                ("pairs", C.c_uint32), ("tiles", C.c_uint32), ("set_size", C.c_uint32)]
 
 
 def _bind_batch():
@@ -191,7 +191,8 @@ class BatchPlan:
         check(L.ipb_batch_plan_groups(self._h, n.value, groups, C.byref(n)))
         return {"kernels": k.value, "tensor_pairs": t.value,
                 "launches": [{"row_width": g.row_width, "tile_rows": g.tile_rows, "masked": bool(g.masked),
-                              "pairs": g.pairs, "tiles": g.tiles} for g in groups[: n.value]]}
+                              "pairs": g.pairs, "tiles": g.tiles, "set_size": g.set_size}
+                             for g in groups[: n.value]]}
 
     def close(self):
         if self._h:

@@ -308,6 +308,7 @@ typedef struct ipb_batch_group {
     int masked;         /* binary-mask launch */
     uint32_t pairs;     /* pairs in the launch */
     uint32_t tiles;     /* tiles the launch's CTAs share */
+    uint32_t set_size;  /* pairs on one image computed together per tile (1..4) */
 } ipb_batch_group;
 ipb_status ipb_batch_plan_groups(const ipb_batch_plan *plan, uint32_t max, ipb_batch_group *out,
                                  uint32_t *count);
@@ -332,6 +333,15 @@ typedef struct ipb_tensor_plan {
     uint32_t smem_bytes;     /* dynamic shared memory per CTA */
 } ipb_tensor_plan;
 ipb_status ipb_tensor_plan_for(uint32_t w, uint32_t h, int masked, int batch, ipb_tensor_plan *out);
+/* The same view for a batch group whose pairs on one image (one template
+ * size, one mask kind) are computed together in sets of problems_per_set
+ * (1..4): a tile's staged image rows and the A operand built from them serve
+ * every member, each with its own template side and accumulators
+ * (tmem_columns counts every member's). Replaces no reference function;
+ * IPB_ERR_INVALID_ARGUMENT when no such plan fits (the batch planner then
+ * computes those pairs alone). */
+ipb_status ipb_tensor_set_plan_for(uint32_t w, uint32_t h, int masked, uint32_t problems_per_set,
+                                   ipb_tensor_plan *out);
 
 /* ---- many templates against one image --------------------------------------
  * match_template (src/template_matching.rs:78-92) of n templates of one size

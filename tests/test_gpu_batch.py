@@ -198,7 +198,10 @@ def test_batch_tuner_persists_choices_and_replays_rearm_extremes(tmp_path, monke
     info = plan.info()
     assert info["kernels"] == len(info["launches"]) + 1  # tensor launches + the extremes finish
     assert info["tensor_pairs"] == len(items)
-    groups = [ln.split() for ln in f.read_text().splitlines() if ln.startswith("group ")]
+    # "group2 ks0 masked h8 wlog mlog set ks nt n": the group key (natural row
+    # width, mask kind, template height, sizes, largest set the pairs form)
+    # and the choice (row width, tile height, problems per set)
+    groups = [ln.split() for ln in f.read_text().splitlines() if ln.startswith("group2 ")]
     assert groups, "group decisions persisted"
     plan.launch()
     torch.cuda.synchronize()
@@ -215,7 +218,7 @@ def test_batch_tuner_persists_choices_and_replays_rearm_extremes(tmp_path, monke
     _check(new_items, batch.outs, batch.extremes_host())
     plan.close()
     # a persisted choice is read back: force 64-row tiles at the natural width
-    f.write_text("".join(f"group {k[1]} {k[2]} {k[3]} {k[4]} {k[5]} {k[1]} 64\n" for k in groups))
+    f.write_text("".join(f"group2 {k[1]} {k[2]} {k[3]} {k[4]} {k[5]} {k[6]} {k[1]} 64 1\n" for k in groups))
     L.ipb_batch_tuning_reset()
     plan2 = device.BatchPlan(batch)
     info2 = plan2.info()
@@ -225,3 +228,76 @@ def test_batch_tuner_persists_choices_and_replays_rearm_extremes(tmp_path, monke
     _check(new_items, batch.outs, batch.extremes_host())
     plan2.close()
     L.ipb_batch_tuning_reset()
+
+
+def _shared_image_items(seed):
+    """Pairs that share images: per image, classes of 1..8 pairs with one
+    template size (own template content, methods, binary masks or none), a
+    class that repeats one template over all four methods, and a second
+    template size on the same image. Odd image sizes, so that tiles are
+    ragged at both edges."""
+    g = np.random.default_rng(seed)
+    items = []
+    for H, W, sizes in [(301, 517, [(64, 64, 8), (20, 33, 3)]), (143, 260, [(48, 48, 5)]),
+                        (90, 1100, [(17, 130, 2), (9, 8, 4)]), (260, 260, [(64, 64, 1)])]:
+        image = g.integers(0, 256, (H, W), dtype=np.uint8)
+        for h, w, count in sizes:
+            for masked in (False, True):
+                if masked and w > 128:
+                    continue
+                for _ in range(count):
+                    template = g.integers(0, 256, (h, w), dtype=np.uint8)
+                    mask = (g.random((h, w)) < 0.8).astype(np.uint8) if masked else None
+                    items.append((image, template, int(g.integers(0, 4)), mask))
+        template = g.integers(0, 256, (32, 40), dtype=np.uint8)
+        for method in range(4):  # one template, every method
+            items.append((image, template, method, None))
+    return items
+
+
+def _to_device_shared(items):
+    """Device tensors with one copy per distinct host array (pairs that share
+    an image share its device buffer, so the planner can form sets)."""
+    import torch
+    cache = {}
+
+    def dev(a):
+        if id(a) not in cache:
+            cache[id(a)] = torch.from_numpy(a).cuda()
+        return cache[id(a)]
+    out = []
+    for image, template, method, mask in items:
+        t = (dev(image), dev(template), method)
+        if mask is not None:
+            t = t + (dev(mask),)
+        out.append(t)
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pairs_sharing_images_form_sets_bit_exact(precision):
+    """Pairs on one image with one template size are computed together
+    (sets of up to four share the image's A rows; each keeps its own
+    template side, accumulators and epilogue): every map and extremes record
+    must equal the oracle's, for both exact precisions, and a replayed plan
+    must give the same again."""
+    import torch
+
+    from imageproc_b200 import device
+    items = _shared_image_items(11 + precision)
+    batch = device.Batch(_to_device_shared(items))
+    plan = device.BatchPlan(batch, precision)
+    for _ in range(2):
+        for out in batch.outs:
+            out.fill_(-1.0)
+        plan.launch()
+        torch.cuda.synchronize()
+        ex = batch.extremes_host()
+        for k, ((image, template, method, mask), out, e) in enumerate(zip(items, batch.outs, ex)):
+            got = out.cpu().numpy()
+            exp = O.match_exact(image, template, method, mask, precision=precision)
+            bad = np.argwhere(bits(got) != bits(exp))
+            assert bad.size == 0, (k, image.shape, template.shape, method, mask is not None, bad[:3])
+            mx, mn, mxl, mnl = O.find_extremes(exp)
+            assert (e.max_value, e.min_value, e.max_value_location, e.min_value_location) == \
+                (float(mx), float(mn), mxl, mnl), k

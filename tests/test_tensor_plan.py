@@ -85,3 +85,40 @@ def test_plans_of_the_headline_shapes():
     assert (mb["tile_rows"], mb["rows_per_stage"], mb["image_buffers"]) == (96, 3, 2)
     ms = _lib.tensor_plan(64, 64, True, batch=False)
     assert (ms["tile_rows"], ms["rows_per_stage"], ms["image_buffers"]) == (64, 4, 2)
+
+
+@pytest.mark.parametrize("masked", [False, True])
+def test_set_plans_within_the_hardware(masked):
+    # pairs on one image are computed in sets of 2..4: every member's
+    # accumulators and template side must fit beside the A stages, and the
+    # kernel's shared-memory header (TSS partials and keys per member slot)
+    # stays below the band table. Where no set plan fits, the planner
+    # computes the pairs alone, which the single-pair plan above covers.
+    planned = 0
+    for w, h, m in shapes():
+        if m != masked or _lib.tensor_plan(w, h, m, batch=True) is None:
+            continue
+        for n in (1, 2, 3, 4):
+            p = _lib.tensor_set_plan(w, h, m, n)
+            if n == 1:
+                assert p is not None, (w, h, m)
+            if p is None:
+                continue
+            planned += 1
+            assert SMEM_ONE_CTA_PER_SM <= p["smem_bytes"] <= SMEM_MAX, (w, h, m, n, p)
+            assert p["tmem_columns"] <= TMEM_COLUMNS, (w, h, m, n, p)
+            assert p["image_rows"] == p["tile_rows"] + h - 1 <= BAND_TABLE_ROWS
+            assert BAND_TABLE_OFFSET + (p["image_rows"] + 3) * 16 <= p["smem_bytes"]
+            assert 1 <= p["rows_per_stage"] <= 16 and p["tile_rows"] % 16 == 0
+    assert planned > 20000
+
+
+def test_set_plans_of_the_headline_shapes():
+    # 64x64 templates: four unmasked maps per set on 64-row tiles (the four
+    # accumulators take 256 columns, 8 image rows per stage); four
+    # binary-mask maps per set on 32-row tiles (2 image rows per stage)
+    p = _lib.tensor_set_plan(64, 64, False, 4)
+    assert (p["tile_rows"], p["rows_per_stage"], p["tmem_columns"]) == (64, 8, 4 * 64 + 2 * 16 * 8)
+    p = _lib.tensor_set_plan(64, 64, True, 4)
+    assert (p["tile_rows"], p["rows_per_stage"], p["tmem_columns"]) == (32, 2, 4 * 2 * 32 + 2 * 3 * 16 * 2)
+    assert _lib.tensor_set_plan(64, 64, False, 5) is None
