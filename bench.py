@@ -191,16 +191,16 @@ def barrier(world: int):
         dist.barrier()
 
 
-def executed_mac_ratio(W: int, H: int, w: int, h: int, masked: bool) -> dict:
-    """MACs the tensor-core kernel issues per algorithmic MAC for one map: per
-    tile of 128 output columns x NT rows, image row r of the tile feeds the
-    16-aligned band of output rows [r - h + 1, r] (tm_umma.cu, the band
-    table), K = w rounded up to 32, one correlation (3 with a binary mask)."""
-    from imageproc_b200 import _lib
-    plan = _lib.tensor_plan(w, h, masked, True)
-    NT = plan["tile_rows"]
+def executed_mac_ratio(W: int, H: int, w: int, h: int, masked: bool, NT: int, set_size: int) -> dict:
+    """MACs the tensor-core kernel issues per algorithmic MAC for one map of a
+    launch with tiles of NT rows and sets of `set_size` maps on one image:
+    per tile of 128 output columns x NT rows, image row r of the tile feeds
+    the 16-aligned band of output rows [r - h + 1, r] (tm_umma.cu, the band
+    table), K = w rounded up to 32; per map one correlation (X), and with a
+    binary mask the two correlations of Y = sum I^2 m, which a set whose
+    members share the mask computes once for all of them."""
     kmma = (w + 31) // 32 * 32
-    ncorr = 3 if masked else 1
+    ncorr = 1 + (2.0 / set_size if masked else 0.0)
     Wo, Ho = W - w + 1, H - h + 1
     tiles_x = (Wo + 127) // 128
     executed = 0
@@ -211,7 +211,7 @@ def executed_mac_ratio(W: int, H: int, w: int, h: int, masked: bool) -> dict:
             n1 = min(NT, (r & ~15) + 16)
             executed += 128 * (n1 - n0) * kmma * ncorr
     executed *= tiles_x
-    return {"tile_rows": NT, "ratio": executed / (Wo * Ho * w * h)}
+    return {"tile_rows": NT, "set_size": set_size, "ratio": executed / (Wo * Ho * w * h)}
 
 
 def cpu_reference_sample(scene, target_s: float, threads: int):
@@ -726,8 +726,9 @@ def run_ours(args, world, rank, local):
                          extremes=False)
     plan = device.BatchPlan(batch, tm.Precision.ExactFp64)
     # the tuned launches: pairs on one image share a tile's A rows in sets
+    step_groups = plan.info()["launches"]
     step_launches = [f"{g['pairs']} {'binary-mask' if g['masked'] else 'unmasked'} maps, tile {g['tile_rows']} "
-                     f"rows, sets of {g['set_size']} ({g['tiles']} tiles)" for g in plan.info()["launches"]]
+                     f"rows, sets of {g['set_size']} ({g['tiles']} tiles)" for g in step_groups]
 
     def step():
         plan.launch(stream)
@@ -818,8 +819,11 @@ def run_ours(args, world, rank, local):
                                     "both launches' MACs / span")
         # the banded-Toeplitz formulation issues more MACs than the algorithmic
         # count: the pipe-level fraction counts the MACs the kernel executes
-        ratios = {"unmasked": executed_mac_ratio(W_IMG, H_IMG, T, T, False),
-                  "binary_mask": executed_mac_ratio(W_IMG, H_IMG, T, T, True)}
+        grp = {bool(g["masked"]): g for g in step_groups}
+        ratios = {"unmasked": executed_mac_ratio(W_IMG, H_IMG, T, T, False, grp[False]["tile_rows"],
+                                                 grp[False]["set_size"]),
+                  "binary_mask": executed_mac_ratio(W_IMG, H_IMG, T, T, True, grp[True]["tile_rows"],
+                                                    grp[True]["set_size"])}
         executed_per_step = MAC_PER_MAP * 4 * (ratios["unmasked"]["ratio"] + ratios["binary_mask"]["ratio"])
         roofline["executed_mac_ratio"] = {k: round(v["ratio"], 4) for k, v in ratios.items()}
         roofline["pipe_frac"] = roofline["frac"] * executed_per_step / MAC_PER_STEP

@@ -198,10 +198,12 @@ struct UmmaProblem {
   uint32_t Wo, Ho, tiles_x, tile_begin;  // tile_begin: first global tile of the problem
   uint32_t kmma, zrows, rows_max, load_mode;
   int method, precision;
-  // Problems on one image with one template size may form a set that the
-  // kernel computes tile by tile together, sharing the staged image rows and
-  // the A operand built from them (each member keeps its own template side,
-  // accumulators, MMAs and epilogue). On a set's first problem: the number of
+  // Problems on one image with one template size (and one mask buffer) may
+  // form a set that the kernel computes tile by tile together, sharing the
+  // staged image rows and the A operand built from them (each member keeps
+  // its own template side, X accumulator, MMAs and epilogue; a masked set's
+  // Y = sum I^2 m, which depends on the image and the mask alone, is
+  // computed once for all members). On a set's first problem: the number of
   // members (1 for a problem alone); 0 on the others, which follow it in the
   // problem list and carry its tile_begin. Tiles are counted per set.
   uint32_t set_n;

@@ -246,7 +246,8 @@ __device__ __forceinline__ void build_stage_rows(const StageRows& sr) {
 // ncols) of the accumulators for its 32 lanes (output columns).
 struct UmmaEpi {
   const UmmaProblem* q;
-  uint32_t tmem, lane_base, c_begin, ncols, NT, nrows, m, x, y0, tss, lane;
+  uint32_t tmem, xcol, ycol;  // tensor memory; the member's X and (masked) the set's Y accumulator columns
+  uint32_t lane_base, c_begin, ncols, NT, nrows, m, x, y0, tss, lane;
   const uint32_t* s_rs;  // unmasked: row sums of squares of the tile's image rows
   uint32_t Y;            // unmasked: window sum of the first column (row c_begin)
 };
@@ -263,13 +264,13 @@ __device__ __forceinline__ void umma_epilogue(const UmmaEpi& e) {
   unsigned long long kmin = ~0ull, kmax = 0ull;
   for (uint32_t n0 = e.c_begin; n0 < e.c_begin + e.ncols; n0 += kEpiCols) {
     uint32_t vx[kEpiCols];
-    tmem_ld8(tmem_addr(e.tmem, e.lane_base, n0), vx);
+    tmem_ld8(tmem_addr(e.tmem, e.lane_base, e.xcol + n0), vx);
     uint32_t yv[kEpiCols];
     if constexpr (MASKED && kMethod == kCcorr) {
 #pragma unroll
       for (int k = 0; k < kEpiCols; ++k) yv[k] = 0u;  // not computed: CrossCorrelation is X alone
     } else if constexpr (MASKED) {
-      tmem_ld8(tmem_addr(e.tmem, e.lane_base, e.NT + n0), yv);
+      tmem_ld8(tmem_addr(e.tmem, e.lane_base, e.ycol + n0), yv);
     } else {
       // window sums of the chunk: loads first, then the sliding chain
       uint32_t add[kEpiCols], subv[kEpiCols];
@@ -364,7 +365,7 @@ __device__ __forceinline__ void umma_epilogue_dispatch(const UmmaEpi& e, int met
 // accumulators over the row's band of output rows.
 struct StageIssue {
   const uint4* band;
-  uint32_t r0, cnt, a_stage, a_row_cols, dlo, dhi, zslot16, zoff1, kstride, ksteps, tmem, acc_cols, NT, ymask;
+  uint32_t r0, cnt, a_stage, a_row_cols, dlo, dhi, zslot16, zoff1, kstride, ksteps, tmem, NT, ycol, ymask;
 };
 
 template <int NS, int KS, bool MASKED>
@@ -380,17 +381,28 @@ __device__ __forceinline__ void issue_stage(const StageIssue& si) {
         const uint32_t n0 = bd[j].x, idesc = bd[j].y;
         const uint32_t zrow = si.dlo + bd[j].z;
         const uint32_t a = si.a_stage + (i0 + j) * si.a_row_cols;
+        // X: each member's own template side into its own accumulator
 #pragma unroll
         for (int p = 0; p < NS; ++p) {
+          const uint32_t zo = zrow + p * si.zslot16;
 #pragma unroll
-          for (int c = 0; c < NCORR; ++c) {
-            if (c > 0 && !((si.ymask >> p) & 1u)) break;  // masked CrossCorrelation: X alone
-            const uint32_t zo = zrow + p * si.zslot16 + c * si.zoff1;
-            const uint32_t acc = p * si.acc_cols + (c == 0 ? 0u : si.NT);  // X, or Y for both parts of I^2
+          for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
+            if (kk < si.ksteps)
+              mma_i8_ts(si.tmem + p * si.NT + n0, a + kk * 8, ((uint64_t)si.dhi << 32) | (zo + kk * si.kstride),
+                        idesc, 1u);
+          }
+        }
+        // Y = sum I^2 m: both parts of I^2 against the members' common mask
+        // (the first member's m and 255 m), once per set, unless every
+        // member is CrossCorrelation (X alone)
+        if (MASKED && si.ymask) {
+#pragma unroll
+          for (int c = 1; c < NCORR; ++c) {
+            const uint32_t zo = zrow + c * si.zoff1;
 #pragma unroll
             for (uint32_t kk = 0; kk < (uint32_t)(KS / 8); ++kk) {
               if (kk < si.ksteps)
-                mma_i8_ts(si.tmem + acc + n0, a + (MASKED ? c * KS : 0) + kk * 8,
+                mma_i8_ts(si.tmem + si.ycol + n0, a + c * KS + kk * 8,
                           ((uint64_t)si.dhi << 32) | (zo + kk * si.kstride), idesc, 1u);
             }
           }
@@ -405,8 +417,6 @@ __device__ __forceinline__ void issue_stage(const StageIssue& si) {
 template <int KS, bool MASKED, bool SETS>
 __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_constant__ UmmaLaunch L) {
   constexpr int NPL = MASKED ? 3 : 1;    // staged image planes: I (, I^2 mod 255, floor(I^2 / 255))
-  constexpr int NCORR = MASKED ? 3 : 1;  // correlations, one per plane
-  constexpr int NACC = MASKED ? 2 : 1;   // accumulators: X (, Y)
   constexpr int NZ = MASKED ? 3 : 1;     // reversed-template buffers, one per correlation
   extern __shared__ __align__(1024) uint8_t smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -453,8 +463,11 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-  const uint32_t acc_cols = NACC * L.NT;  // accumulator columns per set member
-  const uint32_t a_col0 = (SETS ? L.set_max : 1u) * acc_cols;
+  // accumulators: X of member p at column p NT; masked, the set's Y (its
+  // members share the image and the mask, so Y = sum I^2 m is theirs in
+  // common) after the members' X; then the A stages
+  const uint32_t ycol = (SETS ? L.set_max : 1u) * L.NT;
+  const uint32_t a_col0 = ycol + (MASKED ? L.NT : 0u);
   const uint32_t a_row_cols = NPL * KS;
 
   uint32_t g = 0;            // pipeline stage fills so far (same count in builders and the MMA warp)
@@ -620,11 +633,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
       const uint32_t ncols = 16 * ((sub + 1) * chunks / kSubs) - c_begin;
       {
         const uint32_t zero16[16] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-        for (uint32_t p = 0; p < nset; ++p)
-#pragma unroll
-          for (int c = 0; c < NACC; ++c)
-            for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
-              tmem_st16(tmem_addr(tmem, lane_base, p * acc_cols + c * L.NT + col), zero16);
+        for (uint32_t p = 0; p <= nset; ++p) {
+          if (p == nset && !MASKED) break;
+          const uint32_t base = p < nset ? p * L.NT : ycol;  // members' X, then the set's Y
+          for (uint32_t col = c_begin; col < c_begin + ncols; col += 16)
+            tmem_st16(tmem_addr(tmem, lane_base, base + col), zero16);
+        }
       }
       for (uint32_t st = 0; st < nst; ++st, ++g) {
         const uint32_t s = g % kStages;
@@ -673,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         // common window sum of I^2, unmasked)
         for (uint32_t p = 0; p < nset; ++p) {
           const UmmaProblem qp = P[pi + p];
-          const UmmaEpi e{&qp, tmem + p * acc_cols, lane_base, c_begin, ncols, L.NT, nrows, m, x, y0, s_tss[p],
+          const UmmaEpi e{&qp, tmem, p * L.NT, ycol, lane_base, c_begin, ncols, L.NT, nrows, m, x, y0, s_tss[p],
                           (uint32_t)lane, s_rs, Y};
           umma_epilogue_dispatch<MASKED>(e, qp.method, qp.precision == IPB_PRECISION_EXACT_FP64, qp.ext != nullptr);
         }
@@ -707,7 +721,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         const uint32_t a_stage = tmem + a_col0 + s * L.rps * a_row_cols;
         if (leader) {
           const StageIssue si{band, r0, cnt, a_stage, a_row_cols, dlo, dhi, zslot16, zoff1, kstride, ksteps,
-                              tmem, acc_cols, L.NT, ymask};
+                              tmem, L.NT, ycol, ymask};
           if constexpr (SETS) {
             switch (nset) {
               case 1: issue_stage<1, KS, MASKED>(si); break;
@@ -792,8 +806,8 @@ uint32_t ks_of(uint32_t w) {
 // nt_only: a tile height the plan must use (0: the tallest that fits).
 // Tile heights, tallest first, for sets of up to `set` problems: a tile of
 // NT output rows reads NT + h - 1 image rows, so taller tiles repeat fewer
-// rows, while each member's accumulators (NT columns, two with a mask) leave
-// less tensor memory for the A stages. Binary-mask tiles of 96 rows (`tall`:
+// rows, while each member's accumulator (NT columns, plus the set's common Y
+// with a mask) leaves less tensor memory for the A stages. Binary-mask tiles of 96 rows (`tall`:
 // launches of many tiles, where throughput counts) only where a stage still
 // holds 3 image rows; a launch of one map or one row band ends after about
 // one tile's time, which the 64-row tile keeps shorter. Sets trade tile
@@ -806,8 +820,8 @@ uint32_t tile_heights(bool masked, bool tall, uint32_t set, uint32_t out[2]) {
     out[0] = masked ? 64u : 128u;
     out[1] = masked ? 32u : 64u;
   } else {
-    out[0] = masked ? 32u : 64u;
-    out[1] = masked ? 16u : 32u;
+    out[0] = 64u;
+    out[1] = 32u;
   }
   return 2;
 }
@@ -815,7 +829,7 @@ uint32_t tile_heights(bool masked, bool tall, uint32_t set, uint32_t out[2]) {
 bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl, uint32_t nt_only = 0,
                uint32_t set = 1) {
   if (set < 1 || set > kMaxSet) return false;
-  const uint32_t npl = masked ? 3 : 1, nacc = masked ? 2 : 1, nz = masked ? 3 : 1;
+  const uint32_t npl = masked ? 3 : 1, nz = masked ? 3 : 1;
   pl.ks = ks;
   pl.masked = masked;
   pl.set_max = set;
@@ -826,8 +840,9 @@ bool make_plan(uint32_t ks, bool masked, uint32_t hmax, bool tall, UmmaPlan& pl,
   tile_heights(masked, tall, set, nts);
   for (uint32_t nt : nts) {
     if (nt_only && nt != nt_only) continue;
-    if (set * nacc * nt >= kTmemCols) continue;
-    const uint32_t tm_left = kTmemCols - set * nacc * nt;
+    const uint32_t acc = (set + (masked ? 1u : 0u)) * nt;  // members' X, the set's Y
+    if (acc >= kTmemCols) continue;
+    const uint32_t tm_left = kTmemCols - acc;
     const uint32_t rps = tm_left / (kStages * npl * ks);
     if (rps < 1) continue;
     if (masked && nt > 64 && rps < 3) continue;
@@ -895,12 +910,12 @@ uint32_t umma_tile_heights(bool masked, uint32_t set, uint32_t out[2]) {
 
 namespace {
 // the class a problem's set is drawn from: one image, one template size, one mask kind
+// (binary-mask sets also share the mask buffer: their Y is common)
 bool same_class(const UmmaProblem& a, const UmmaProblem& b) {
-  return a.img == b.img && a.W == b.W && a.H == b.H && a.w == b.w && a.h == b.h &&
-         (a.mask != nullptr) == (b.mask != nullptr);
+  return a.img == b.img && a.W == b.W && a.H == b.H && a.w == b.w && a.h == b.h && a.mask == b.mask;
 }
 bool class_less(const UmmaProblem& a, const UmmaProblem& b) {
-  return std::tie(a.img, a.W, a.H, a.w, a.h) < std::tie(b.img, b.W, b.H, b.w, b.h);
+  return std::tie(a.img, a.W, a.H, a.w, a.h, a.mask) < std::tie(b.img, b.W, b.H, b.w, b.h, b.mask);
 }
 }  // namespace
 
@@ -1118,7 +1133,7 @@ IPB_API ipb_status ipb_tensor_set_plan_for(uint32_t w, uint32_t h, int masked, u
   out->rows_per_stage = pl.rps;
   out->stages = kStages;
   out->image_buffers = pl.nbuf;
-  out->tmem_columns = problems_per_set * accumulators * pl.NT + kStages * planes * pl.ks * pl.rps;
+  out->tmem_columns = (problems_per_set + accumulators - 1) * pl.NT + kStages * planes * pl.ks * pl.rps;
   out->smem_bytes = pl.smem;
   return IPB_OK;
 }

@@ -233,9 +233,9 @@ def test_batch_tuner_persists_choices_and_replays_rearm_extremes(tmp_path, monke
 def _shared_image_items(seed):
     """Pairs that share images: per image, classes of 1..8 pairs with one
     template size (own template content, methods, binary masks or none), a
-    class that repeats one template over all four methods, and a second
-    template size on the same image. Odd image sizes, so that tiles are
-    ragged at both edges."""
+    class that repeats one template over all four methods, a second template
+    size on the same image, and binary-mask classes that share one mask
+    buffer. Odd image sizes, so that tiles are ragged at both edges."""
     g = np.random.default_rng(seed)
     items = []
     for H, W, sizes in [(301, 517, [(64, 64, 8), (20, 33, 3)]), (143, 260, [(48, 48, 5)]),
@@ -252,6 +252,18 @@ def _shared_image_items(seed):
         template = g.integers(0, 256, (32, 40), dtype=np.uint8)
         for method in range(4):  # one template, every method
             items.append((image, template, method, None))
+        # binary-mask pairs sharing one mask buffer (their sets compute the
+        # common Y = sum I^2 m once): mixed methods, then CrossCorrelation
+        # alone (no Y at all)
+        for count, methods in ((6, None), (3, 2)):
+            mask = (g.random((24, 36)) < 0.7).astype(np.uint8)
+            for _ in range(count):
+                template = g.integers(0, 256, (24, 36), dtype=np.uint8)
+                method = int(g.integers(0, 4)) if methods is None else methods
+                items.append((image, template, method, mask))
+        template = g.integers(0, 256, (24, 36), dtype=np.uint8)
+        for method in range(4):  # one template and one mask, every method
+            items.append((image, template, method, mask))
     return items
 
 

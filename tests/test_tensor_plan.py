@@ -116,9 +116,10 @@ def test_set_plans_within_the_hardware(masked):
 def test_set_plans_of_the_headline_shapes():
     # 64x64 templates: four unmasked maps per set on 64-row tiles (the four
     # accumulators take 256 columns, 8 image rows per stage); four
-    # binary-mask maps per set on 32-row tiles (2 image rows per stage)
+    # binary-mask maps per set on 64-row tiles (four X accumulators and the
+    # set's common Y, 2 image rows of 3 planes per stage)
     p = _lib.tensor_set_plan(64, 64, False, 4)
     assert (p["tile_rows"], p["rows_per_stage"], p["tmem_columns"]) == (64, 8, 4 * 64 + 2 * 16 * 8)
     p = _lib.tensor_set_plan(64, 64, True, 4)
-    assert (p["tile_rows"], p["rows_per_stage"], p["tmem_columns"]) == (32, 2, 4 * 2 * 32 + 2 * 3 * 16 * 2)
+    assert (p["tile_rows"], p["rows_per_stage"], p["tmem_columns"]) == (64, 2, 5 * 64 + 2 * 3 * 16 * 2)
     assert _lib.tensor_set_plan(64, 64, False, 5) is None
