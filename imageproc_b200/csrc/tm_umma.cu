@@ -214,31 +214,32 @@ __device__ __forceinline__ uint32_t build_row(const uint8_t* plane_row, uint32_t
   return rs;
 }
 
-// One builder warp's rows of a pipeline stage: rows r_first, r_first +
-// kSubs, ... below r_end, each row's planes into its tensor-memory columns;
-// unmasked, the lanes' row sums of squares go to s_rs[r][m].
+// One builder warp's share of a pipeline stage's A rows [r0, r_end): rows
+// r_first, r_first + kSubs, ... unmasked, with the lanes' row sums of
+// squares into s_rs[r][m]; with a mask the stage's (row, plane) builds are
+// dealt out over the quadrant's kSubs warps in turn, so that stages of few
+// image rows (sets) keep every builder warp busy.
 struct StageRows {
   const uint8_t* img_buf;
-  uint32_t r_first, r_end, r0, tcol0, a_row_cols, imgp, plane_bytes, lane, m, w, tmem;
+  uint32_t r_first, r_end, r0, tcol0, a_row_cols, imgp, plane_bytes, lane, m, w, tmem, sub;
   uint32_t* s_rs;
   bool need_y;
 };
 
 template <int KS, bool MASKED, int Q>
 __device__ __forceinline__ void build_stage_rows(const StageRows& sr) {
-  constexpr int NPL = MASKED ? 3 : 1;
-  for (uint32_t r = sr.r_first; r < sr.r_end; r += kSubs) {
-    const uint32_t ta = tmem_addr(sr.tmem, Q * 32, sr.tcol0 + (r - sr.r0) * sr.a_row_cols);
-    const uint8_t* row = sr.img_buf + r * sr.imgp;
-    if constexpr (MASKED) {
-      build_row<KS, false, Q>(row, sr.lane, sr.w, ta);
-      if (sr.need_y) {
-#pragma unroll
-        for (int pl = 1; pl < NPL; ++pl) build_row<KS, false, Q>(row + pl * sr.plane_bytes, sr.lane, sr.w, ta + pl * KS);
-      }
-    } else {
-      sr.s_rs[r * kM + sr.m] = build_row<KS, true, Q>(row, sr.lane, sr.w, ta);
+  if constexpr (MASKED) {
+    const uint32_t npl = sr.need_y ? 3u : 1u;
+    const uint32_t items = (sr.r_end - sr.r0) * npl;
+    for (uint32_t t = sr.sub; t < items; t += kSubs) {
+      const uint32_t i = t / npl, pl = t % npl;
+      build_row<KS, false, Q>(sr.img_buf + (sr.r0 + i) * sr.imgp + pl * sr.plane_bytes, sr.lane, sr.w,
+                              tmem_addr(sr.tmem, Q * 32, sr.tcol0 + i * sr.a_row_cols + pl * KS));
     }
+  } else {
+    for (uint32_t r = sr.r_first; r < sr.r_end; r += kSubs)
+      sr.s_rs[r * kM + sr.m] = build_row<KS, true, Q>(sr.img_buf + r * sr.imgp, sr.lane, sr.w,
+                                                      tmem_addr(sr.tmem, Q * 32, sr.tcol0 + (r - sr.r0) * sr.a_row_cols));
   }
 }
 
@@ -654,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_match_kernel(const __grid_co
         // compile-time word offset of the lanes' windows (warp-uniform)
         const StageRows sr{img_buf, r0 + ((sub + kSubs - (r0 % kSubs)) % kSubs), r_end, r0,
                            a_col0 + s * L.rps * a_row_cols, a_row_cols, L.imgp, L.plane_bytes,
-                           (uint32_t)lane, m, q.w, tmem, s_rs, need_y};
+                           (uint32_t)lane, m, q.w, tmem, sub, s_rs, need_y};
         switch (q4) {
           case 0: build_stage_rows<KS, MASKED, 0>(sr); break;
           case 1: build_stage_rows<KS, MASKED, 1>(sr); break;
