@@ -657,6 +657,13 @@ def run_next_rows(args, world, rank, local) -> dict:
         "workload": f"value_noise {side}x{side} u8, 5x5 f32 kernel, clamped to u8", "ms": ms,
         "gpix_per_s": world * side * side / (ms / 1e3) / 1e9,
         "roofline": roof(2 * side * side, ms, "filter_clamped_u8_4096_k5"),
+        # the reference's per-tap multiply and add, each rounded (no fused
+        # multiply-add): 2 f32 instructions per tap against one per lane and
+        # cycle (no measured f32 figure: 148 SMs x 128 lanes at the max clock)
+        "compute_roofline": {"bound": "f32", "achieved": 2.0 * 25 * side * side / (ms / 1e3) / 1e12,
+                             "peak": 148 * 128 * 1.965e9 / 1e12, "unit": "TFLOP/s",
+                             "frac": 2.0 * 25 * side * side / (ms / 1e3) / (148 * 128 * 1.965e9),
+                             "peak_source": "nominal: 148 SMs x 128 f32 lanes x 1965 MHz, one mul or add each"},
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "512 of 4096 rows, oracle restatement of src/filter/mod.rs:29-70, scaled by rows"}}
     del d_f, d_k
@@ -678,6 +685,11 @@ def run_next_rows(args, world, rank, local) -> dict:
         "workload": f"{n} points uniform on {side}x{side}, f32 scores, radius 8 ({len(kept)} kept)",
         "ms": ms, "mpoints_per_s": world * n / (ms / 1e3) / 1e6,
         "api": "ipb_local_maxima (host arrays in and out, copies inside the time)",
+        # algorithmic bytes: the points in (x, y, score: 12 B each) and the kept
+        # indices out; the call is launch- and latency-bound (a sort, scans, the
+        # reference's per-point scan and a compaction, plus two copies)
+        "roofline": {**roof(12 * n + 4 * len(kept), ms, "local_maxima_100k"),
+                     "note": "launch- and latency-bound: host arrays, about ten launches and two copies per call"},
         "cpu_baseline": {"ms": cpu_ms, "cores": 1, "kind": "port",
                          "sample": "all points, oracle restatement of src/suppress.rs:111-173"}}
 
