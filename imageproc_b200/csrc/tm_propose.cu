@@ -466,42 +466,70 @@ constexpr int kTile = 64;  // origins per table tile side (16 x 16 micro blocks)
 
 __global__ void __launch_bounds__(256) micro_table_kernel(const uint8_t* __restrict__ img, uint32_t W, uint32_t H,
                                                           uint32_t Mx, uint32_t My, uint32_t* __restrict__ micro) {
-  __shared__ uint8_t s_img[kTile + kBlk - 1][kTile + kBlk - 1 + 1];
-  __shared__ uint16_t s_row[kTile + kBlk - 1][kTile];
+  constexpr uint32_t kIn = kTile + kBlk - 1;  // 75 image rows and columns per tile
+  constexpr uint32_t kRun = 16;               // box sums per thread along a row or a column
+  __shared__ uint8_t s_img[kIn][kIn + 1];
+  __shared__ uint16_t s_row[kIn][kTile];      // 12-pixel row sums at each origin column
   const uint32_t qx0 = blockIdx.x * kTile, qy0 = blockIdx.y * kTile;
   const uint32_t Qx = W - kBlk + 1, Qy = H - kBlk + 1;  // box-sum origins
-  constexpr uint32_t kIn = kTile + kBlk - 1;            // 75
   for (uint32_t i = threadIdx.x; i < kIn * kIn; i += blockDim.x) {
     const uint32_t r = i / kIn, c = i % kIn, y = qy0 + r, x = qx0 + c;
     s_img[r][c] = (y < H && x < W) ? img[(size_t)y * W + x] : 0;
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < kIn * kTile; i += blockDim.x) {
-    const uint32_t r = i / kTile, c = i % kTile;
+  // row sums: each thread slides a 12-pixel window over a run of 16 columns
+  for (uint32_t i = threadIdx.x; i < kIn * (kTile / kRun); i += blockDim.x) {
+    const uint32_t r = i / (kTile / kRun), c0 = (i % (kTile / kRun)) * kRun;
     uint32_t v = 0;
 #pragma unroll
-    for (int d = 0; d < kBlk; ++d) v += s_img[r][c + d];
-    s_row[r][c] = (uint16_t)v;
-  }
-  __syncthreads();
-  // thread = micro block (16 x 16 per tile): 4 columns of 4 box sums each
-  const uint32_t mxl = threadIdx.x & 15, myl = threadIdx.x >> 4;
-  const uint32_t mx = blockIdx.x * 16 + mxl, my = blockIdx.y * 16 + myl;
-  if (mx >= Mx || my >= My) return;
-  uint32_t mn = 0xFFFFu, mxv = 0u;
-  for (uint32_t c = 4 * mxl; c < 4 * mxl + 4; ++c) {
-    if (qx0 + c >= Qx) break;
-    const uint32_t r0 = 4 * myl;
-    uint32_t v = 0;
+    for (int d = 0; d < kBlk; ++d) v += s_img[r][c0 + d];
+    s_row[r][c0] = (uint16_t)v;
 #pragma unroll
-    for (int d = 0; d < kBlk; ++d) v += s_row[r0 + d][c];
-    for (uint32_t r = r0; r < r0 + 4 && qy0 + r < Qy; ++r) {
-      if (r > r0) v += (uint32_t)s_row[r + kBlk - 1][c] - (uint32_t)s_row[r - 1][c];
-      mn = v < mn ? v : mn;
-      mxv = v > mxv ? v : mxv;
+    for (uint32_t j = 1; j < kRun; ++j) {
+      v += (uint32_t)s_img[r][c0 + j + kBlk - 1] - (uint32_t)s_img[r][c0 + j - 1];
+      s_row[r][c0 + j] = (uint16_t)v;
     }
   }
-  micro[(size_t)my * Mx + mx] = mn | (mxv << 16);
+  __syncthreads();
+  // box sums: thread (column c, rows 16 g .. 16 g + 15) slides down its
+  // column; each run covers four micro blocks, whose minimum and maximum
+  // over their 4 columns are folded across 4 adjacent lanes
+  const uint32_t c = threadIdx.x & (kTile - 1), g = threadIdx.x / kTile;
+  const bool col_ok = qx0 + c < Qx;
+  uint32_t v = 0;
+#pragma unroll
+  for (int d = 0; d < kBlk; ++d) v += s_row[kRun * g + d][c];
+  uint32_t mn[4], mx[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    mn[k] = 0xFFFFu;
+    mx[k] = 0u;
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < kRun; ++j) {
+    const uint32_t r = kRun * g + j;
+    if (j > 0) v += (uint32_t)s_row[r + kBlk - 1][c] - (uint32_t)s_row[r - 1][c];
+    if (col_ok && qy0 + r < Qy) {
+      mn[j / 4] = min(mn[j / 4], v);
+      mx[j / 4] = max(mx[j / 4], v);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+      mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+    }
+  }
+  const uint32_t mxb = blockIdx.x * (kTile / 4) + c / 4;
+  if ((c & 3u) == 0 && mxb < Mx) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t myb = blockIdx.y * (kTile / 4) + 4 * g + k;
+      if (myb < My) micro[(size_t)myb * Mx + mxb] = mn[k] | (mx[k] << 16);
+    }
+  }
 }
 
 // out[m] = min / max of in over the 4 x 4 entries in[m + step * (a, b)],
