@@ -203,10 +203,148 @@ __global__ void __launch_bounds__(256) snm_cols_tile_kernel(const T* __restrict_
   }
 }
 
+// One-pass form for element types of 4 bytes or less and radii up to 16: a
+// block owns 128 output columns x 32 output rows, stages the keys of that
+// tile and its r halo once, and runs both window passes in shared memory.
+// Each element's rank is one 64-bit word, (key << 32) | (0xFFFF - col) << 16 |
+// (0xFFFF - row) in tile-local coordinates, so the plain maximum is the
+// reference's winner (largest value, then smaller x, then smaller y) and 0
+// stands for the clipped-away cells outside the image. Both passes find
+// window maxima by van Herk / Gil-Werman: a thread owns k = 2r + 1
+// consecutive outputs, keeps the suffix maxima of their first inputs in
+// registers and sweeps the prefix maxima of the next k, so each output
+// costs two maxima whatever the radius (instead of a scan of 2r + 1).
+constexpr uint32_t kFusedTW = 128, kFusedTH = 32, kFusedThreads = 256;
+
+template <uint32_t KMAX, typename In, typename Emit>
+__device__ __forceinline__ void vhgw_run(uint32_t k, uint32_t n_in, uint32_t n_out, const uint32_t base,
+                                         uint64_t (&h)[KMAX], const In& in, const Emit& emit) {
+  // suffix maxima of inputs base .. base + k - 1
+  uint64_t run = 0;
+#pragma unroll
+  for (int t = KMAX - 1; t >= 0; --t)
+    if ((uint32_t)t < k) {
+      const uint32_t c = base + t;
+      const uint64_t v = c < n_in ? in(c) : 0ull;
+      run = v > run ? v : run;
+      h[t] = run;
+    }
+  // prefix maxima of inputs base + k .. base + 2k - 2, merged into the outputs
+  run = 0;
+#pragma unroll
+  for (uint32_t t = 0; t < KMAX; ++t)
+    if (t < k) {
+      const uint32_t o = base + t;
+      if (o < n_out) emit(o, h[t] > run ? h[t] : run);
+      const uint32_t c = base + k + t;
+      const uint64_t v = c < n_in ? in(c) : 0ull;
+      run = v > run ? v : run;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T from_okey(uint32_t k) {
+  if constexpr (std::is_same<T, float>::value) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+  } else if constexpr (std::is_signed<T>::value) {
+    return (T)(int32_t)(k ^ 0x80000000u);
+  } else {
+    return (T)k;
+  }
+}
+
+template <typename T, uint32_t KMAX>
+__global__ void __launch_bounds__(kFusedThreads) snm_fused_kernel(const T* __restrict__ img, uint32_t W, uint32_t H,
+                                                                  uint32_t r, T* __restrict__ out) {
+  static_assert(sizeof(T) <= 4, "32-bit keys");
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  const uint32_t k = 2 * r + 1;
+  const uint32_t ic = kFusedTW + 2 * r, ir = kFusedTH + 2 * r;
+  uint64_t* s_row = reinterpret_cast<uint64_t*>(s_raw);            // [ir][kFusedTW] row-window winners
+  uint32_t* s_key = reinterpret_cast<uint32_t*>(s_row + ir * kFusedTW);  // [ir][ic] keys
+  const long long x0 = (long long)blockIdx.x * kFusedTW, y0 = (long long)blockIdx.y * kFusedTH;
+  const long long gx0 = x0 - r, gy0 = y0 - r;
+  // stage the keys; cells outside the image are never read as keys (their
+  // rank is 0, decided from the coordinates)
+  for (uint32_t idx = threadIdx.x; idx < ir * ic; idx += kFusedThreads) {
+    const uint32_t i = idx / ic, c = idx - i * ic;
+    const long long gy = gy0 + i, gx = gx0 + c;
+    uint32_t key = 0;
+    if (gy >= 0 && gy < (long long)H && gx >= 0 && gx < (long long)W) key = okey(img[(size_t)gy * W + gx]);
+    s_key[idx] = key;
+  }
+  __syncthreads();
+  // row pass: for tile-local row i and output column o, the winner of input
+  // columns o .. o + 2r
+  const uint32_t nseg = (kFusedTW + k - 1) / k;
+  const long long col_lo = -gx0, col_hi = (long long)W - gx0;  // local columns inside the image
+  for (uint32_t task = threadIdx.x; task < ir * nseg; task += kFusedThreads) {
+    const uint32_t i = task / nseg, seg = task - i * nseg;
+    const long long gy = gy0 + i;
+    const bool row_in = gy >= 0 && gy < (long long)H;
+    const uint32_t* kr = s_key + i * ic;
+    const uint64_t rowbits = 0xFFFFu - i;
+    uint64_t h[KMAX];
+    vhgw_run<KMAX>(
+        k, ic, kFusedTW, seg * k, h,
+        [&](uint32_t c) -> uint64_t {
+          if (!row_in || (long long)c < col_lo || (long long)c >= col_hi) return 0ull;
+          return ((uint64_t)kr[c] << 32) | ((uint64_t)(0xFFFFu - c) << 16) | rowbits;
+        },
+        [&](uint32_t o, uint64_t v) { s_row[i * kFusedTW + o] = v; });
+  }
+  __syncthreads();
+  // column pass: for output (o, j), the winner of row winners j .. j + 2r of
+  // column o; the pixel keeps its value iff it is that winner
+  const uint32_t nseg2 = (kFusedTH + k - 1) / k;
+  for (uint32_t task = threadIdx.x; task < kFusedTW * nseg2; task += kFusedThreads) {
+    const uint32_t o = task % kFusedTW, seg = task / kFusedTW;
+    const long long gx = x0 + o;
+    if (gx >= (long long)W) continue;
+    uint64_t h[KMAX];
+    vhgw_run<KMAX>(
+        k, ir, kFusedTH, seg * k, h, [&](uint32_t i) -> uint64_t { return s_row[i * kFusedTW + o]; },
+        [&](uint32_t j, uint64_t v) {
+          const long long gy = y0 + j;
+          if (gy >= (long long)H) return;
+          const uint32_t own = ((0xFFFFu - (o + r)) << 16) | (0xFFFFu - (j + r));
+          out[(size_t)gy * W + gx] = (uint32_t)v == own ? from_okey<T>((uint32_t)(v >> 32)) : T(0);
+        });
+  }
+}
+
+size_t snm_fused_smem(uint32_t r) {
+  return (size_t)(kFusedTH + 2 * r) * (kFusedTW * 8 + (kFusedTW + 2 * r) * 4);
+}
+
+template <typename T, uint32_t KMAX>
+cudaError_t launch_snm_fused(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, cudaStream_t s) {
+  static PerDeviceOnce attr;
+  cudaError_t e = attr.run([] {
+    return cudaFuncSetAttribute(snm_fused_kernel<T, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)snm_fused_smem((KMAX - 1) / 2));
+  });
+  if (e != cudaSuccess) return e;
+  const dim3 grid((W + kFusedTW - 1) / kFusedTW, (H + kFusedTH - 1) / kFusedTH);
+  snm_fused_kernel<T, KMAX><<<grid, kFusedThreads, snm_fused_smem(r), s>>>(img, W, H, r, out);
+  count_launch(kKernelSuppress);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_snm_t(const T* img, uint32_t W, uint32_t H, uint32_t r, T* out, void* scratch, cudaStream_t s) {
   using K = KeyOf<T>;
   if (W == 0 || H == 0) return cudaSuccess;
+  // the one-pass form reads neighbouring tiles' pixels, so it needs an output
+  // apart from the image; tiles are counted in 16 bits (rows of grid.y)
+  if constexpr (sizeof(T) <= 4) {
+    const bool apart = (const void*)img != (const void*)out;
+    if (apart && r <= 16 && (H + kFusedTH - 1) / kFusedTH <= 65535u) {
+      if (r <= 4) return launch_snm_fused<T, 9>(img, W, H, r, out, s);
+      if (r <= 8) return launch_snm_fused<T, 17>(img, W, H, r, out, s);
+      return launch_snm_fused<T, 33>(img, W, H, r, out, s);
+    }
+  }
   uint32_t* bx = static_cast<uint32_t*>(scratch);
   K* bk = reinterpret_cast<K*>(static_cast<uint8_t*>(scratch) + align_up((size_t)W * H * 4, 256));
   const size_t band = (size_t)kRowBand * (kRowThreads + 2 * (size_t)r) * sizeof(K);

@@ -139,6 +139,39 @@ def test_suppress_golden_and_edges():
     assert sp.suppress_non_maximum(np.zeros((0, 5), np.uint8), 3).shape == (0, 5)
 
 
+@pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.float32])
+def test_suppress_one_pass_tiles_and_two_pass_radii(dtype):
+    # radii 0..16 take the one-pass tile kernel (128 x 32 tiles, so these maps
+    # cross tile edges in both directions); 17 and 40 the two-pass kernels
+    g = np.random.default_rng(21)
+    for r in (0, 1, 4, 5, 8, 9, 12, 16, 17, 40):
+        H, W = int(g.integers(33, 200)), int(g.integers(129, 420))
+        a = g.integers(0, 7, (H, W)).astype(dtype)  # many ties across tiles
+        assert np.array_equal(sp.suppress_non_maximum(a, r), O.suppress_non_maximum(a, r)), (H, W, r)
+
+
+def test_suppress_device_in_place():
+    # an output that is the image itself runs the two-pass kernels, which read
+    # each pixel only where they write it
+    import ctypes as C
+
+    import torch
+
+    from imageproc_b200 import _lib
+    L = _lib.lib()
+    L.ipb_suppress_non_maximum_f32_device.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                      C.c_void_p, C.c_void_p]
+    L.ipb_suppress_non_maximum_f32_device.restype = C.c_int
+    g = np.random.default_rng(22)
+    a = g.standard_normal((97, 300)).astype(np.float32)
+    exp = O.suppress_non_maximum(a, 6)
+    d = torch.from_numpy(a).cuda()
+    stream = torch.cuda.current_stream().cuda_stream or None
+    _lib.check(L.ipb_suppress_non_maximum_f32_device(d.data_ptr(), 300, 97, 6, d.data_ptr(), stream))
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), exp.view(np.uint32))
+
+
 def test_suppress_wide_radius_and_large_image():
     g = np.random.default_rng(11)
     a = g.integers(0, 6, (50, 40)).astype(np.uint16)
