@@ -96,7 +96,7 @@ const char* kernel_name(int id) {
   static const char* names[kKernelCount] = {
       "template_prep", "integral_rows", "integral_cols", "exact_cc",
       "template_sum_f32", "reference_f32", "find_extremes", "umma_i8", "many_i8", "suppress", "filter",
-      "example", "proposal_net", "propose"};
+      "example", "proposal_net", "propose", "rows_i8", "window_sq_sums"};
   return id >= 0 && id < kKernelCount ? names[id] : "unknown";
 }
 
@@ -143,12 +143,14 @@ int precision_from_env() {
 std::atomic<int> g_precision{precision_from_env()};
 
 // Kernel family for exact matches: 0 = choose (tensor cores where the shape
-// allows), 1 = CUDA cores only, 2 = tensor cores wherever supported.
+// allows), 1 = CUDA cores only, 2 = tensor cores wherever supported (the
+// Hankel-row kernel), 3 = the row-operand tensor kernel wherever it applies.
 int path_from_env() {
   const char* v = std::getenv("IPB_PATH");
   if (!v) return 0;
   if (!std::strcmp(v, "1") || !std::strcmp(v, "cuda_core")) return 1;
   if (!std::strcmp(v, "2") || !std::strcmp(v, "tensor")) return 2;
+  if (!std::strcmp(v, "3") || !std::strcmp(v, "row_operand")) return 3;
   return 0;
 }
 std::atomic<int> g_path{path_from_env()};
@@ -341,9 +343,15 @@ ipb_status run_match(Context* c, const MatchArgs& a) {
     return IPB_OK;
   }
   const bool ref = a.precision == IPB_PRECISION_REFERENCE_F32;
-  const bool tensor = !ref && g_path.load() != 1 && umma_supported(a);
+  const int path = g_path.load();
+  const bool rows = !ref && path == 3 && shift_supported(a);
+  const bool tensor = !ref && !rows && path != 1 && umma_supported(a);
   ipb_status st;
-  if (tensor) {
+  if (rows) {
+    if ((st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true)) ||
+        (st = ensure(c, c->scratch, shift_scratch_bytes(a))))
+      return st;
+  } else if (tensor) {
     if ((st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
   } else {
     const size_t need = ref ? reference_scratch_bytes(a) : exact_cc_scratch_bytes(a);
@@ -353,7 +361,11 @@ ipb_status run_match(Context* c, const MatchArgs& a) {
   MatchArgs la = a;
   la.timer = acquire_timer();
   cudaError_t e;
-  if (tensor) {
+  if (rows) {
+    c->tag += 1;
+    c->tensor_since_check = true;
+    e = launch_shift(la, c->scratch.p, nullptr, static_cast<unsigned int*>(c->errw.p), c->tag);
+  } else if (tensor) {
     c->tag += 1;
     c->tensor_since_check = true;
     e = launch_umma(la, static_cast<unsigned int*>(c->errw.p), c->tag);
@@ -524,8 +536,9 @@ ipb_status host_match_banded(Context* c, const MatchArgs& full, const uint8_t* i
                              const uint8_t* mask, uint32_t nb, float* out) {
   ipb_status st;
   if ((st = ensure_band_streams(c, nb))) return st;
+  const int path = g_path.load();
   const bool side_by_side =
-      full.precision != IPB_PRECISION_REFERENCE_F32 && g_path.load() != 1 && umma_supported(full);
+      full.precision != IPB_PRECISION_REFERENCE_F32 && path != 1 && path != 3 && umma_supported(full);
   if (side_by_side && (st = ensure(c, c->errw, sizeof(unsigned int), /*zero=*/true))) return st;
   // A copy into page-locked memory returns at once, so a band's score rows are
   // queued as soon as its launch is: they cross while the host still copies
@@ -842,7 +855,7 @@ IPB_API void ipb_debug_set_pipeline_wait_ns(uint64_t ns) {
 }
 
 IPB_API ipb_status ipb_set_path(int path) {
-  if (path < 0 || path > 2) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown kernel path");
+  if (path < 0 || path > 3) return fail(IPB_ERR_INVALID_ARGUMENT, "unknown kernel path");
   g_path.store(path);
   return IPB_OK;
 }

@@ -46,6 +46,7 @@ struct ipb_batch_plan {
   std::vector<ipb::MatchArgs> args;  // per pair, device pointers
   std::vector<ipb_extremes_f32*> ext_out;
   std::vector<bool> tensor;
+  std::vector<unsigned long long*> key_of;  // fused extremes keys per pair, or null
   struct Group {
     ipb::UmmaPlan plan;
     std::vector<uint32_t> members;
@@ -54,6 +55,13 @@ struct ipb_batch_plan {
     uint32_t tiles = 0;
   };
   std::vector<Group> groups;
+  // unmasked pairs of one template on the row-operand kernel: up to 8 per
+  // launch, with the template blocks and window sums in the group's scratch
+  struct RowGroup {
+    std::vector<uint32_t> members;
+    void* d_scratch = nullptr;
+  };
+  std::vector<RowGroup> rgroups;
   // fused extremes of tensor pairs: keys {min, max}, map widths, output records
   unsigned long long* d_keys = nullptr;
   uint32_t* d_widths = nullptr;
@@ -325,6 +333,8 @@ void release(ipb_batch_plan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   for (auto& g : p->groups)
     if (g.d_probs) cudaFree(g.d_probs);
+  for (auto& g : p->rgroups)
+    if (g.d_scratch) cudaFree(g.d_scratch);
   for (void* b : {(void*)p->d_keys, (void*)p->d_widths, (void*)p->d_outs, p->d_scratch, p->d_ext_scratch,
                   (void*)p->d_ext_result, (void*)p->d_err, (void*)p->d_sched})
     if (b) cudaFree(b);
@@ -339,7 +349,7 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
   uint32_t k = 0;  // the keys were armed at creation and are re-armed by the finish kernel
   // groups after the first run on the side stream, between a fork and a join
   // on s; concurrent launches are timed as one span on s
-  const bool side_by_side = p->groups.size() >= 2 && p->side;
+  const bool side_by_side = p->groups.size() + p->rgroups.size() >= 2 && p->side;
   KernelTimer* span = timed && side_by_side ? acquire_kernel_timer() : nullptr;
   double span_macs = 0, span_bytes = 0;
   if (span) {
@@ -380,6 +390,34 @@ ipb_status enqueue(ipb_batch_plan* p, cudaStream_t s, bool timed, uint32_t* kern
     span_macs += macs;
     span_bytes += bytes;
     ++k;
+  }
+  for (size_t ri = 0; ri < p->rgroups.size() && launch_err == cudaSuccess; ++ri) {
+    const ipb_batch_plan::RowGroup& g = p->rgroups[ri];
+    const cudaStream_t gs = side_by_side && (ri > 0 || !p->groups.empty()) ? p->side : s;
+    std::vector<MatchArgs> probs;
+    std::vector<unsigned long long*> ext;
+    double macs = 0, bytes = 0;
+    for (uint32_t i : g.members) {
+      probs.push_back(p->args[i]);
+      ext.push_back(p->key_of[i]);
+      const MatchArgs& a = p->args[i];
+      const double Wo = a.W - a.w + 1.0, Ho = a.H - a.h + 1.0, tp = (double)a.w * a.h;
+      macs += Wo * Ho * tp;
+      bytes += (double)a.W * a.H + tp + 4.0 * Wo * Ho;
+    }
+    KernelTimer* t = timed && !side_by_side ? acquire_kernel_timer() : nullptr;
+    launch_err = launch_shift_multi(probs.data(), ext.data(), (uint32_t)probs.size(), g.d_scratch, p->d_err,
+                                    p->tag, gs, t);
+    if (launch_err != cudaSuccess) break;
+    if (t) note_kernel_timed(t, macs, bytes);
+    span_macs += macs;
+    span_bytes += bytes;
+    // template blocks, one window-sum map per image, the matching launch
+    std::vector<const uint8_t*> imgs;
+    for (const MatchArgs& a : probs)
+      if (a.method != IPB_CROSS_CORRELATION && std::find(imgs.begin(), imgs.end(), a.img) == imgs.end())
+        imgs.push_back(a.img);
+    k += 2 + (uint32_t)imgs.size();
   }
   if (side_by_side) {
     // joined on every path, a failed launch included, so that s orders all of
@@ -472,10 +510,17 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
   // kernel family per pair, then tensor groups keyed by (row width, masked)
   const int tune = autotune_mode();
   std::map<uint32_t, std::vector<uint32_t>> by_key;
+  // unmasked pairs the row-operand kernel takes, by template (pointer and size)
+  std::map<std::tuple<const uint8_t*, uint32_t, uint32_t>, std::vector<uint32_t>> by_tpl;
   for (uint32_t i = 0; i < n; ++i) {
     MatchArgs a = p->args[i];
     if (!a.w || !a.h) continue;
     a.stream = nullptr;
+    if (shift_preferred(a)) {
+      p->tensor[i] = true;
+      by_tpl[std::make_tuple(a.tpl, a.w, a.h)].push_back(i);
+      continue;
+    }
     if (choose_tensor(a, tune == 2, p->d_scratch, p->d_err)) {
       p->tensor[i] = true;
       by_key[umma_group_key(a)].push_back(i);
@@ -508,6 +553,20 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
     if ((e = cudaMemset(p->d_sched, 0, sched_bytes)) != cudaSuccess) return fail(to_status(e, "cudaMemset"));
   }
   auto keys_of = [&](uint32_t i) { return slot[i] >= 0 ? p->d_keys + 2 * slot[i] : nullptr; };
+  p->key_of.resize(n);
+  for (uint32_t i = 0; i < n; ++i) p->key_of[i] = keys_of(i);
+  for (auto& kv : by_tpl)
+    for (size_t b = 0; b < kv.second.size(); b += kShiftMaxProblems) {
+      ipb_batch_plan::RowGroup g;
+      g.members.assign(kv.second.begin() + b,
+                       kv.second.begin() + std::min(kv.second.size(), b + (size_t)kShiftMaxProblems));
+      std::vector<MatchArgs> probs;
+      for (uint32_t i : g.members) probs.push_back(p->args[i]);
+      if ((e = cudaMalloc(&g.d_scratch, shift_multi_scratch_bytes(probs.data(), (uint32_t)probs.size()))) !=
+          cudaSuccess)
+        return fail(to_status(e, "cudaMalloc"));
+      p->rgroups.push_back(std::move(g));
+    }
   // the largest set the pairs `mem` form (pairs on one image with one
   // template size), within the set cap
   auto set_of = [&](const std::vector<uint32_t>& mem) {
@@ -597,7 +656,7 @@ ipb_status create(const ipb_pair* pairs, uint32_t n, int precision, bool capture
                      if (x.plan.masked != y.plan.masked) return x.plan.masked;
                      return x.plan.ks > y.plan.ks;
                    });
-  if (p->groups.size() >= 2) {
+  if (p->groups.size() + p->rgroups.size() >= 2) {
     if ((e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming)) != cudaSuccess)

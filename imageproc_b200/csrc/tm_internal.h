@@ -72,6 +72,8 @@ enum KernelId : int {
   kKernelExample,
   kKernelLearned,
   kKernelPropose,
+  kKernelRows,
+  kKernelWindowSq,
   kKernelCount
 };
 const char* kernel_name(int id);
@@ -186,6 +188,25 @@ cudaError_t launch_exact_cc(const MatchArgs& a, void* scratch);
 // later one failed.
 bool umma_supported(const MatchArgs& a);
 cudaError_t launch_umma(const MatchArgs& a, unsigned int* err_word, unsigned int tag);
+
+// ---- tensor-core exact kernel with the image row as the A operand (tm_shift.cu)
+// Unmasked exact matches of images whose width is a multiple of 16 (rows
+// 16-byte aligned); scratch = shift_scratch_bytes (the window sums of I^2,
+// none for CrossCorrelation). ext: fused find_extremes keys {min, max} (armed
+// by the caller) or null.
+bool shift_supported(const MatchArgs& a);
+// shift_supported and chosen by the kernel path setting (ipb_set_path)
+bool shift_preferred(const MatchArgs& a);
+size_t shift_scratch_bytes(const MatchArgs& a);
+cudaError_t launch_shift(const MatchArgs& a, void* scratch, unsigned long long* ext, unsigned int* err_word,
+                         unsigned int tag);
+// Up to 8 problems with one template (same pointer and size) in one launch,
+// each with its own extremes keys (ext[i], or ext null); problems on one image
+// share its window sums. scratch = shift_multi_scratch_bytes.
+constexpr uint32_t kShiftMaxProblems = 8;
+size_t shift_multi_scratch_bytes(const MatchArgs* a, uint32_t n);
+cudaError_t launch_shift_multi(const MatchArgs* a, unsigned long long* const* ext, uint32_t n, void* scratch,
+                               unsigned int* err_word, unsigned int tag, cudaStream_t stream, KernelTimer* timer);
 
 // One problem of a tensor-core launch (device-side descriptor).
 struct UmmaProblem {
@@ -315,6 +336,6 @@ void count_launches(unsigned long long n);
 bool profiling_enabled();
 KernelTimer* acquire_kernel_timer();
 void note_kernel_timed(KernelTimer* t, double macs, double bytes);
-int kernel_path();  // 0 auto, 1 CUDA cores, 2 tensor cores
+int kernel_path();  // 0 auto, 1 CUDA cores, 2 tensor cores, 3 row-operand kernel
 
 }  // namespace ipb

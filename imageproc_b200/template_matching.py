@@ -75,6 +75,7 @@ class Path(enum.IntEnum):
     Auto = 0
     CudaCores = 1
     TensorCores = 2
+    RowOperand = 3
 
 
 def set_path(path: Path | int) -> None:

@@ -124,7 +124,9 @@ int ipb_get_precision(void);
 
 /* Kernel family of the exact precisions (no counterpart in the reference):
  * 0 = automatic (tcgen05 tensor cores where the template shape allows, else
- * CUDA cores), 1 = CUDA cores only, 2 = tensor cores wherever supported.
+ * CUDA cores), 1 = CUDA cores only, 2 = tensor cores wherever supported,
+ * 3 = the tensor-core kernel that reads image rows as its A operand
+ * (unmasked, image width a multiple of 16) wherever it applies, else as 0.
  * Results are identical; the switch exists for testing and measurement.
  * Initial value from the environment variable IPB_PATH (0/1/2 or
  * auto/cuda_core/tensor). */
