@@ -39,9 +39,10 @@
 // (two per tensor-memory lane quadrant, four tile rows each) drain each
 // finished tile from one of
 // two accumulator buffers of 128 columns while the MMAs of the next tile run.
-// Every wait is bounded; a wait that runs out records the launch's tag in the
-// error word and the CTA leaves its loops, drains its MMAs and frees its
-// tensor memory.
+// Every wait is bounded (a budget per tile, so the global timer is read once
+// per tile on the fast path, not once per row); a wait that runs out records
+// the launch's tag in the error word and the CTA leaves its loops, drains its
+// MMAs and frees its tensor memory.
 #include <algorithm>
 
 #include "tm_common.cuh"
@@ -309,10 +310,12 @@ __global__ void __launch_bounds__(kThreads, 1) shift_match_kernel(const __grid_c
       const TileCoord t = tile_coord(L, tile);
       const ShiftProblem& pr = L.p[t.p];
       const uint32_t chunks = min(L.rowbytes, pr.W - t.x0) / 16;  // W is a multiple of 16
+      // one budget per tile: the global timer is read once here, not per row
+      const unsigned long long deadline = global_ns() + L.wait_ns;
       bool ok = true;
       for (uint32_t rho = 0; rho < t.nrows; ++rho) {
         const uint32_t slot = q % L.stages, u = q / L.stages;
-        if (u > 0 && !mbar_wait(empty + slot, (u - 1) & 1, global_ns() + L.wait_ns)) {
+        if (u > 0 && !mbar_wait(empty + slot, (u - 1) & 1, deadline)) {
           if (lane == 0) {
             atomicMax(L.err, L.tag);
             *s_flag = 1;
@@ -357,7 +360,9 @@ __global__ void __launch_bounds__(kThreads, 1) shift_match_kernel(const __grid_c
     for (uint32_t tile = blockIdx.x; tile < L.tiles && ok; tile += G, ++it) {
       const TileCoord t = tile_coord(L, tile);
       const uint32_t buf = it & 1, v = it >> 1;
-      if (v > 0 && !mbar_wait(acc_empty + buf, (v - 1) & 1, global_ns() + L.wait_ns)) {
+      // one budget per tile: the global timer is read once here, not per row
+      const unsigned long long deadline = global_ns() + L.wait_ns;
+      if (v > 0 && !mbar_wait(acc_empty + buf, (v - 1) & 1, deadline)) {
         ok = false;
         break;
       }
@@ -367,7 +372,7 @@ __global__ void __launch_bounds__(kThreads, 1) shift_match_kernel(const __grid_c
                      idesc_u8u8_s32(kLanes, kAccCols), 0u);
       for (uint32_t rho = 0; rho < t.nrows; ++rho, ++q) {
         const uint32_t slot = q % L.stages, u = q / L.stages;
-        if (!mbar_wait(full + slot, u & 1, global_ns() + L.wait_ns)) {
+        if (!mbar_wait(full + slot, u & 1, deadline)) {
           ok = false;
           break;
         }
