@@ -81,6 +81,7 @@ struct ShiftProblem {
 };
 
 constexpr uint32_t kMaxProblems = 8;
+static_assert(kMaxProblems == kShiftMaxProblems, "problems per launch");
 
 struct ShiftLaunch {
   ShiftProblem p[kMaxProblems];
