@@ -24,7 +24,8 @@
 // of j = j_lo .. j_hi (the output rows that image row feeds) are consecutive,
 // starting at block h - 1 - (rho - j_lo); the MMA's N is 16 (j_hi - j_lo + 1)
 // and its accumulator columns start at 16 j_lo, so no zero rows are issued.
-// A first MMA with a zero A operand clears the tile's accumulator.
+// A first MMA with zero operands (a zeroed buffer read through the same
+// overlapping descriptor) clears the tile's accumulator.
 //
 // Y = sum I^2 over each window (SumOfSquaredErrors and the normalised
 // methods) comes from a window-sum map built beforehand by two separable
@@ -34,11 +35,13 @@
 //
 // Pipeline: one loader warp copies each image row segment (2048 + K bytes,
 // less at the image's right edge) with 16-byte cp.async copies into a ring of
-// shared-memory slots, several rows in flight, one warp issues the MMAs of a row
-// once its slot is full and commits the slot back, and eight epilogue warps
+// shared-memory slots, two loader warps taking the rows in turn with several
+// in flight each; one warp issues the MMAs of a
+// row once its slot is full and commits the slot back; eight epilogue warps
 // (two per tensor-memory lane quadrant, four tile rows each) drain each
-// finished tile from one of
-// two accumulator buffers of 128 columns while the MMAs of the next tile run.
+// finished tile from one of two accumulator buffers of 128 columns while the
+// MMAs of the next tile run. The template blocks arrive by bulk copies once
+// per CTA.
 // Every wait is bounded (a budget per tile, so the global timer is read once
 // per tile on the fast path, not once per row); a wait that runs out records
 // the launch's tag in the error word and the CTA leaves its loops, drains its
@@ -59,8 +62,9 @@ constexpr uint32_t kTileW = kLanes * 16;    // output columns per tile
 constexpr uint32_t kNT = 8;                 // output rows per tile (N = 128)
 constexpr uint32_t kAccCols = kNT * 16;     // accumulator columns per buffer
 constexpr uint32_t kStages = 16;            // image-row slots at most (8 at least)
-constexpr uint32_t kEpiWarps = 8, kMmaWarp = 8, kLoadWarp = 9;
-constexpr uint32_t kThreads = 10 * 32;
+constexpr uint32_t kEpiWarps = 8, kMmaWarp = 8, kLoadWarp = 9, kLoadWarps = 2;
+constexpr uint32_t kThreads = (kLoadWarp + kLoadWarps) * 32;
+constexpr int kRowsInFlight = 3;  // per loader warp; kLoadWarps x kRowsInFlight < the slots
 // the zero operands of the clearing MMA: A (128 rows) and B (256 rows) both
 // read through the overlapping descriptor, 16 bytes per row
 constexpr uint32_t kZeroBytes = 16 * (kAccCols - 1) + 32 + 16;
@@ -87,7 +91,7 @@ struct ShiftLaunch {
   ShiftProblem p[kMaxProblems];
   uint32_t nprobs, tiles;
   const uint8_t* blocks;  // h blocks of 16 K bytes, then TSS (u32)
-  uint32_t h, K, rowbytes, stages, batch;  // batch: rows per loader hand-off, 3 batches < stages
+  uint32_t h, K, rowbytes, stages;
   uint32_t ring_off, b_off;
   unsigned int* err;
   unsigned int tag;
@@ -297,15 +301,18 @@ __global__ void __launch_bounds__(kThreads, 1) shift_match_kernel(const __grid_c
   const uint32_t tbase = *s_tmem;
   const uint32_t G = gridDim.x;
 
-  if (warp == kLoadWarp) {
-    // ---- loader: each image row segment as 16-byte cp.async copies spread
-    // over the warp, committed in groups of L.batch rows. Once three groups
-    // are in flight the oldest is handed to the MMA warp: every lane waits
-    // for its copies of it (wait_group), makes them visible to the tensor
-    // core's proxy, and after the warp has synchronised one lane arrives on
-    // the group's rows. One proxy fence per group instead of one per row.
-    uint32_t q = 0, handed = 0;
-    const uint32_t batch = L.batch;
+  if (warp >= kLoadWarp) {
+    // ---- loaders: kLoadWarps warps take the image rows in turn (row q to
+    // warp q % kLoadWarps); a row is 16-byte cp.async copies spread over the
+    // warp, committed as one group. A warp keeps kRowsInFlight of its rows in
+    // flight and hands the oldest to the MMA warp: every lane waits for its
+    // copies of it (wait_group), makes them visible to the tensor core's
+    // proxy, and after the warp has synchronised one lane arrives on the row.
+    // Slots and phases advance by increments (no divisions per row).
+    const uint32_t lw = warp - kLoadWarp;
+    uint32_t q = 0, mine = 0, handed = 0;  // rows seen; this warp's rows issued and handed
+    uint32_t slot = 0, u = 0;              // slot of row q and its use count
+    uint32_t hq[kRowsInFlight + 1];        // this warp's rows not yet handed (ring)
     for (uint32_t tile = blockIdx.x; tile < L.tiles && !*reinterpret_cast<volatile uint32_t*>(s_flag);
          tile += G) {
       const TileCoord t = tile_coord(L, tile);
@@ -315,43 +322,46 @@ __global__ void __launch_bounds__(kThreads, 1) shift_match_kernel(const __grid_c
       const unsigned long long deadline = global_ns() + L.wait_ns;
       bool ok = true;
       for (uint32_t rho = 0; rho < t.nrows; ++rho) {
-        const uint32_t slot = q % L.stages, u = q / L.stages;
-        if (u > 0 && !mbar_wait(empty + slot, (u - 1) & 1, deadline)) {
-          if (lane == 0) {
-            atomicMax(L.err, L.tag);
-            *s_flag = 1;
+        if (q % kLoadWarps == lw) {
+          if (u > 0 && !mbar_wait(empty + slot, (u - 1) & 1, deadline)) {
+            if (lane == 0) {
+              atomicMax(L.err, L.tag);
+              *s_flag = 1;
+            }
+            ok = false;
+            break;
           }
-          ok = false;
-          break;
-        }
-        // bytes of the slot past the image row keep whatever they held: an
-        // output column x < Wo reads image bytes x .. x + w - 1 <= W - 1 only,
-        // every other byte of its K window meets a zero of B, and the columns
-        // x >= Wo that do read them are never stored
-        const uint32_t dst = smem_u32(ring + slot * L.rowbytes);
-        const uint8_t* src = pr.img + (size_t)(t.y0 + rho) * pr.W + t.x0;
-        for (uint32_t c = lane; c < chunks; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
-        ++q;
-        if (q % batch == 0) {
+          // bytes of the slot past the image row keep whatever they held: an
+          // output column x < Wo reads image bytes x .. x + w - 1 <= W - 1
+          // only, every other byte of its K window meets a zero of B, and the
+          // columns x >= Wo that do read them are never stored
+          const uint32_t dst = smem_u32(ring + slot * L.rowbytes);
+          const uint8_t* src = pr.img + (size_t)(t.y0 + rho) * pr.W + t.x0;
+          for (uint32_t c = lane; c < chunks; c += 32) cp_async16(dst + 16 * c, src + 16 * c);
           cp_async_commit();
-          if (q - handed >= 3 * batch) {
-            cp_async_wait_group<2>();
+          hq[mine % (kRowsInFlight + 1)] = slot;
+          ++mine;
+          if (mine - handed > kRowsInFlight) {
+            cp_async_wait_group<kRowsInFlight>();
             fence_proxy_async_smem();
             __syncwarp();
-            if (lane == 0)
-              for (uint32_t i = 0; i < batch; ++i) mbar_arrive(full + (handed + i) % L.stages);
-            handed += batch;
+            if (lane == 0) mbar_arrive(full + hq[handed % (kRowsInFlight + 1)]);
+            ++handed;
           }
+        }
+        ++q;
+        if (++slot == L.stages) {
+          slot = 0;
+          ++u;
         }
       }
       if (!ok) break;
     }
-    cp_async_commit();
     cp_async_wait_all();
     fence_proxy_async_smem();
     __syncwarp();
     if (lane == 0)
-      for (; handed < q; ++handed) mbar_arrive(full + handed % L.stages);
+      for (; handed < mine; ++handed) mbar_arrive(full + hq[handed % (kRowsInFlight + 1)]);
   } else if (warp == kMmaWarp) {
     // ---- MMA issue
     uint32_t q = 0, it = 0;
@@ -670,7 +680,6 @@ cudaError_t launch_shift_multi(const MatchArgs* a, unsigned long long* const* ex
   L.rowbytes = kTileW + K;
   L.ring_off = kRingOff;
   L.stages = shift_stages(w, h);
-  L.batch = L.stages >= 13 ? 4u : 2u;
   L.b_off = kRingOff + L.stages * L.rowbytes;
   L.err = err;
   L.tag = tag;
