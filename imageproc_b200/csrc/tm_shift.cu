@@ -622,6 +622,8 @@ size_t shift_scratch_bytes(const MatchArgs& a) { return shift_multi_scratch_byte
 cudaError_t launch_shift_multi(const MatchArgs* a, unsigned long long* const* ext, uint32_t n, void* scratch,
                                unsigned int* err, unsigned int tag, cudaStream_t stream, KernelTimer* timer) {
   if (n == 0 || n > kMaxProblems) return cudaErrorInvalidValue;
+  for (uint32_t i = 1; i < n; ++i)  // one template side per launch
+    if (a[i].tpl != a[0].tpl || a[i].w != a[0].w || a[i].h != a[0].h) return cudaErrorInvalidValue;
   static PerDeviceOnce attr;
   cudaError_t e = attr.run([] {
     cudaError_t r = cudaFuncSetAttribute(shift_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
