@@ -126,3 +126,17 @@ def test_cpp_mirror_raises_reference_panics(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.strip() == "ok"
+
+
+def test_kernel_path_round_trip():
+    # host-side switch only: no kernel runs
+    old = tm.get_path()
+    try:
+        for p in tm.Path:
+            tm.set_path(p)
+            assert tm.get_path() == p
+        assert int(tm.Path.RowOperand) == 3
+        with pytest.raises(ValueError):
+            tm.set_path(4)
+    finally:
+        tm.set_path(old)
