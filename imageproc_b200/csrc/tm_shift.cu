@@ -65,8 +65,8 @@ constexpr uint32_t kStages = 16;            // image-row slots at most (8 at lea
 constexpr uint32_t kEpiWarps = 8, kMmaWarp = 8, kLoadWarp = 9, kLoadWarps = 2;
 constexpr uint32_t kThreads = (kLoadWarp + kLoadWarps) * 32;
 constexpr int kRowsInFlight = 3;  // per loader warp; kLoadWarps x kRowsInFlight < the slots
-// the zero operands of the clearing MMA: A (128 rows) and B (256 rows) both
-// read through the overlapping descriptor, 16 bytes per row
+// the zero operands of the clearing MMA: A (128 rows) and B (kAccCols rows),
+// both read through the overlapping descriptor, 16 bytes per row
 constexpr uint32_t kZeroBytes = 16 * (kAccCols - 1) + 32 + 16;
 constexpr uint32_t kHeader = 1024;  // barriers and flags
 constexpr uint32_t kZeroRegion = (kZeroBytes + 127) / 128 * 128;
